@@ -1,0 +1,361 @@
+"""Benchmark: FP64 CSR SpMV HBM throughput on the large irregular matrix.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sbb|reference]
+                    [--kernel merge|vector|tiled|auto] [--workload c2|c3|c1]
+
+Workload (default): the 5.5M-row irregular matrix (c2_circuit_5.5M: m = n =
+5.5M, nnz ~ 60M, diagonal + band + power-law long-range entries, 550 dense
+rows up to 1,000,000 nnz; val, x, y ~ U(-1,1); alpha = 1, beta = 0.5),
+synthetic and seeded (the reference's SuiteSparse inputs are not available).
+
+One step = one y = alpha*A*x + beta*y over the whole matrix with the data
+resident in HBM.  ``value`` is algorithmic bytes / device time in GB/s,
+bytes = 12*nnz + 4*(m+1) + 8*n + 16*m.  The working set (~874 MB) is larger
+than L2 (126 MB), so no flush is done between steps.  ``e2e`` is the same
+metric through the reference-facing C ABI (spMV_mgpu_v1, kernel 2) with host
+buffers in pinned memory: every step copies the matrix, x and y to the GPU and
+y back.  Multi-GPU runs are independent replicas (one per rank, no
+collective); ``value`` sums the ranks' bytes over the slowest rank's time.
+
+``--impl reference`` times the reference's host CSR SpMV (main.cu:350-356,
+restated with +beta*y in oracle/sbb_oracle.c) on all host cores over a bounded
+sample of the same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sparse-blas_b200"))
+
+import numpy as np  # noqa: E402
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def algo_bytes(m, n, nnz):
+    return 12 * nnz + 4 * (m + 1) + 8 * n + 16 * m
+
+
+def make_workload(name):
+    from sbb import gen
+    if name == "c2":
+        A = gen.c2()
+        x = gen.uniform_vec(21, A.n)
+        y = gen.uniform_vec(22, A.m)
+        return A, x, y, 1.0, 0.5, "c2_circuit_5.5M: m=n=5,500,000, 550 dense rows (max 1,000,000 nnz), alpha=1, beta=0.5"
+    if name == "c3":
+        A = gen.c3()
+        x = gen.uniform_vec(31, A.n)
+        return A, x, np.zeros(A.m), 1.0, 0.0, "c3_shortwide: 4,284 x 1,092,610, lognormal rows (mean 2,640), val=1, alpha=1, beta=0"
+    if name == "c1":
+        A = gen.c1()
+        x = gen.uniform_vec(11, A.n)
+        return A, x, np.zeros(A.m), 1.0, 0.0, "c1_powerlaw_10k: n=10,000, power-law rows, alpha=1, beta=0"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return PEAKS_FALLBACK["hbm_gbs"], "fallback"
+
+
+def traffic_from_profile(kernel_tag, workload):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_tag}_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return int(float(line.split(":", 1)[1].strip()))
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.2)
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "out", "") or "").splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample_time(A, x, y, alpha, beta, threads, budget_s=12.0):
+    """Seconds per full pass of the reference's host loop (bounded sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    rp = np.ascontiguousarray(A.rowptr)
+    reps, t_total = 0, 0.0
+    # first pass also warms the page cache
+    O.spmv_host(rp, A.col, A.val, x, alpha, beta, y, threads)
+    while t_total < budget_s and reps < 50:
+        t0 = time.perf_counter()
+        O.spmv_host(rp, A.col, A.val, x, alpha, beta, y, threads)
+        t_total += time.perf_counter() - t0
+        reps += 1
+    return t_total / reps, reps
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    A, x, y, alpha, beta, desc = make_workload(args.workload)
+    threads = os.cpu_count() or 1
+    sec, reps = cpu_sample_time(A, x, y, alpha, beta, threads, budget_s=args.cpu_budget)
+    gbs = algo_bytes(A.m, A.n, A.nnz) / sec / 1e9
+    line = {
+        "metric": "SpMV HBM GB/s (FP64 CSR, algorithmic bytes 12*nnz+4*(m+1)+8*n+16*m)",
+        "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": reps, "warmup": 1, "ms_per_step": round(sec * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": desc, "nnz": A.nnz, "threads": threads},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"{reps} full passes of the host CSR loop (main.cu:350-356 "
+                                   f"restated with +beta*y, OpenMP static over rows)"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_sbb(args, ws, rank, local):
+    import ctypes as C
+    import torch
+    from sbb._lib import lib
+    from sbb.device import Plan
+    from sbb import api
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    A, x_h, y_h, alpha, beta, desc = make_workload(args.workload)
+    m, n, nnz = A.m, A.n, A.nnz
+    bytes_step = algo_bytes(m, n, nnz)
+
+    rp = torch.from_numpy(A.rowptr32()).to(dev)
+    col = torch.from_numpy(A.col).to(dev)
+    val = torch.from_numpy(A.val).to(dev)
+    x = torch.from_numpy(x_h).to(dev)
+    y0 = torch.from_numpy(y_h).to(dev)
+    y = y0.clone()
+    kw = {}
+    if args.kernel == "merge":
+        kw = dict(items_per_thread=args.ipt, persistent=args.persistent)
+    P = Plan(rp, col, val, n, kernel=args.kernel, **kw)
+    info = P.info()
+    launches = lib().sbb_plan_launches(P.h)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    # warm-up
+    for _ in range(args.warmup):
+        P.spmv(x, y, alpha, beta)
+    torch.cuda.synchronize()
+    P.check()
+
+    # timed region: whole steps (value) and the main kernel alone (roofline)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(ws)
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for i in range(args.steps):
+            rc = lib().sbb_spmv_timed(P.h, alpha, C.c_void_p(x.data_ptr()), beta,
+                                      C.c_void_p(y.data_ptr()), sp,
+                                      C.c_void_p(starts[i].cuda_event),
+                                      C.c_void_p(stops[i].cuda_event))
+            assert rc == 0
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+    P.check()
+    ms_total = t0.elapsed_time(t1)
+    ms_step = max_over_ranks(ms_total / args.steps, ws)
+    kern_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    kern_avg = statistics.mean(kern_ms)
+    value = ws * bytes_step / (ms_step * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    achieved = bytes_step / (kern_avg * 1e-3) / 1e9
+    tag = {1: "vector_kernel", 2: "merge_kernel", 3: "tiled_kernel"}[info["kernel"]]
+    traffic = traffic_from_profile(tag, args.workload)
+
+    # e2e through the reference-facing C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        rp64, colp, valp, xp = pin(A.rowptr), pin(A.col), pin(A.val), pin(x_h)
+        yp = pin(y_h.copy())
+        for _ in range(2):
+            yp[:] = y_h
+            assert api.spMV_mgpu_v1(m, n, nnz, alpha, valp, rp64, colp, xp, beta, yp, 1, 2) == 0
+        e_steps = max(3, min(args.steps, 10))
+        barrier(ws)
+        torch.cuda.synchronize()
+        tt = time.perf_counter()
+        for _ in range(e_steps):
+            rc = api.spMV_mgpu_v1(m, n, nnz, alpha, valp, rp64, colp, xp, beta, yp, 1, 2)
+            assert rc == 0
+        e_sec = (time.perf_counter() - tt) / e_steps
+        e_sec = max_over_ranks(e_sec, ws)
+        h2d = 8 * (m + 1) + 4 * nnz + 8 * nnz + 8 * n + (8 * m if beta != 0 else 0)
+        e2e = {"value": round(ws * bytes_step / e_sec / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * m,
+               "ms_per_step": round(e_sec * 1e3, 3),
+               "api": "spMV_mgpu_v1(kernel=2) host pointers, pinned"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        sec, reps = cpu_sample_time(A, x_h, y_h, alpha, beta, threads, budget_s=args.cpu_budget)
+        cpu = {"value": round(bytes_step / sec / 1e9, 3), "unit": "GB/s", "cores": threads,
+               "kind": "port",
+               "sample": f"{reps} full passes of the host CSR loop over this matrix "
+                         f"(main.cu:350-356 restated with +beta*y; OpenMP static)"}
+
+    if rank == 0:
+        line = {
+            "metric": "SpMV HBM GB/s (FP64 CSR, algorithmic bytes 12*nnz+4*(m+1)+8*n+16*m)",
+            "value": round(value, 3), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "m": m, "n": n, "nnz": nnz,
+                       "kernel": tag, "plan": {k: info[k] for k in
+                                               ("items_per_thread", "persistent", "tile_sigma",
+                                                "vector_width", "tiles")},
+                       "l2": "inputs larger than L2 (working set %.0f MB), no flush" % (bytes_step / 1e6),
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "kernel_ms_avg": round(kern_avg, 5),
+                         "algorithmic_bytes_per_launch": bytes_step},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    P.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="sbb", choices=["sbb", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--kernel", default="merge", choices=["merge", "vector", "tiled", "auto"])
+    ap.add_argument("--ipt", type=int, default=8)
+    ap.add_argument("--persistent", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_sbb(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+/*
+ * sbb_spmv.h — C ABI of libsbb: FP64 CSR SpMV  y = alpha*A*x + beta*y  on one
+ * NVIDIA B200 (sm_100a).
+ *
+ * Part 1 is the drop-in boundary: the entry points of JieyangChen7/Sparse-BLAS
+ * with their exact argument lists, meanings and return codes (citations are
+ * to that project, paths relative to its root).  Part 2 is the device API
+ * (device-resident arrays, reusable plans) the drop-in is built on.
+ *
+ * All functions are extern "C" and take plain pointers and sizes.  Return
+ * codes of the drop-in entry points follow the reference: 0 success,
+ * -1 bad argument / insufficient device memory / kernel failure,
+ *  1 CUDA allocation failure.  Device-API functions return SBB_OK (0) or a
+ * negative SBB_ERR_*; sbb_last_error() gives the message.
+ */
+#ifndef SBB_SPMV_H
+#define SBB_SPMV_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================= Part 1: drop-in boundary ======================== */
+
+/* Replaces spMV_mgpu_baseline (SparseBLAS/include/spmv_kernel.h:9-13,
+ * SparseBLAS/src/dspmv_mgpu_baseline.cu:14-213).  Host pointers; rows split
+ * evenly over ngpu parts, which is pinned to 1 here (ngpu <= 0 -> -1). */
+int spMV_mgpu_baseline(int m, int n, long long nnz, double *alpha,
+                       double *csrVal, long long *csrRowPtr, int *csrColIndex,
+                       double *x, double *beta, double *y, int ngpu);
+
+/* Replaces spMV_mgpu_v1 (SparseBLAS/include/spmv_kernel.h:14-19,
+ * SparseBLAS/src/dspmv_mgpu_v1.cu:16-277).  nnz-balanced split (pinned to one
+ * part), kernel 1 = vector CSR, 2 = merge path, 3 = CSR5-style tiles. */
+int spMV_mgpu_v1(int m, int n, long long nnz, double *alpha, double *csrVal,
+                 long long *csrRowPtr, int *csrColIndex, double *x,
+                 double *beta, double *y, int ngpu, int kernel);
+
+/* Replaces spMV_mgpu_v2 (SparseBLAS/include/spmv_kernel.h:21-28,
+ * SparseBLAS/src/dspmv_mgpu_v2.cu:33-207).  ceil(nnz/nb) tasks with the
+ * reference's split-row merge; the task pool runs as one persistent kernel
+ * with q resident CTAs per SM.  Returns 0 on success (the reference returns
+ * no value, :207). */
+int spMV_mgpu_v2(int m, int n, long long nnz, double *alpha, double *csrVal,
+                 long long *csrRowPtr, int *csrColIndex, double *x,
+                 double *beta, double *y, int ngpu, int kernel, long long nb,
+                 int q);
+
+/* Replaces csr5_kernel (SparseBLAS/include/spmv_kernel.h:4-7,
+ * SparseBLAS/src/csr5_kernel.cu:12-32).  DEVICE pointers, int32 row pointer.
+ * Unlike the reference, alpha and beta are honoured
+ * (the reference drops them: include/detail/cuda/csr5_spmv_cuda.h:22,
+ * include/anonymouslib_cuda.h:281) and the caller's col/val are not modified. */
+int csr5_kernel(int m, int n, int nnz, double *alpha, double *csrVal,
+                int *csrRowPtr, int *csrColIndex, double *x, double *beta,
+                double *y);
+
+/* Replaces get_row_from_index (SparseBLAS/src/spmv_helper.cu:16-39). */
+int get_row_from_index(int n, long long *a, long long idx);
+/* Replaces get_time (SparseBLAS/src/spmv_helper.cu:41-48): wall clock, s. */
+double get_time(void);
+/* Replaces get_gpu_availble_mem (SparseBLAS/src/spmv_helper.cu:51-76):
+ * free memory in GB, minimum over the first ngpu devices that exist. */
+double get_gpu_availble_mem(int ngpu);
+
+/* ========================= Part 2: device API ============================ */
+
+enum {
+    SBB_OK = 0,
+    SBB_ERR_ARG = -1,      /* bad argument                              */
+    SBB_ERR_CUDA = -2,     /* CUDA runtime error                        */
+    SBB_ERR_INPUT = -3,    /* malformed CSR found by a device check     */
+    SBB_ERR_NOMEM = -4     /* allocation failed / would not fit          */
+};
+
+enum {
+    SBB_KERNEL_AUTO = 0,
+    SBB_KERNEL_VECTOR = 1, /* K1: V lanes per row, warp-shuffle reduce   */
+    SBB_KERNEL_MERGE = 2,  /* K2: merge-path split of rows+nnz over CTAs */
+    SBB_KERNEL_TILED = 3   /* K3: CSR5-style 32 x sigma tiles            */
+};
+
+typedef struct {
+    int kernel;            /* SBB_KERNEL_*                                  */
+    int vector_width;      /* K1: 2,4,8,16,32 (0 = from mean row length)    */
+    int items_per_thread;  /* K2: merge items per thread (0 = default)      */
+    int persistent;        /* K2: >0 = persistent CTAs per SM with a device
+                              work queue; 0 = one CTA per tile              */
+    int tile_sigma;        /* K3: nnz per lane per tile (0 = CSR5 rule)     */
+} sbb_config;
+
+typedef struct sbb_plan_s *sbb_plan_t;
+
+typedef struct {
+    int kernel, vector_width, items_per_thread, persistent, tile_sigma;
+    int tiles;             /* K2/K3 work tiles                               */
+    int max_row_len, empty_rows;
+    size_t scratch_bytes;  /* device memory the plan owns                    */
+} sbb_plan_info;
+
+/* Build a plan for an m x n CSR matrix resident on the current device
+ * (int32 row pointer with rowptr[0] == 0 and rowptr[m] == nnz, int32 columns,
+ * FP64 values).  The arrays must stay valid and unchanged while the plan
+ * lives.  cfg may be NULL (automatic choice).  stream: a cudaStream_t or
+ * NULL.  The row pointer is validated (one synchronisation). */
+int sbb_plan_create(sbb_plan_t *plan, int m, int n, int nnz,
+                    const int *d_rowptr, const int *d_col, const double *d_val,
+                    const sbb_config *cfg, void *stream);
+/* FP32-storage form: values (and x at run time) stored as float, each row
+ * segment accumulated in FP32 with compensated (TwoSum) summation, segment
+ * carries combined and alpha/beta applied in FP64. */
+int sbb_plan_create_f32(sbb_plan_t *plan, int m, int n, int nnz,
+                        const int *d_rowptr, const int *d_col,
+                        const float *d_val, const sbb_config *cfg, void *stream);
+/* y = alpha*A*x + beta*y on the stream (asynchronous).  y is not read when
+ * beta == 0.  Out-of-range column indices are skipped and flagged; see
+ * sbb_plan_check. */
+int sbb_spmv(sbb_plan_t plan, double alpha, const double *d_x, double beta,
+             double *d_y, void *stream);
+int sbb_spmv_f32(sbb_plan_t plan, double alpha, const float *d_x, double beta,
+                 double *d_y, void *stream);
+/* sbb_spmv that also records ev_start / ev_stop (cudaEvent_t, may be NULL)
+ * on the stream immediately before and after the plan's main kernel, so the
+ * caller can time that kernel alone (the ordered carry fix-up and the
+ * empty-row pass run after ev_stop). */
+int sbb_spmv_timed(sbb_plan_t plan, double alpha, const void *d_x, double beta,
+                   double *d_y, void *stream, void *ev_start, void *ev_stop);
+/* Number of kernel launches one sbb_spmv of this plan makes. */
+int sbb_plan_launches(sbb_plan_t plan);
+/* Synchronise the plan's status word: SBB_OK or SBB_ERR_INPUT. */
+int sbb_plan_check(sbb_plan_t plan);
+int sbb_plan_info_get(sbb_plan_t plan, sbb_plan_info *info);
+/* Copy the merge-path tile coordinates (tiles+1 rows and nnz offsets) to the
+ * host; returns the number of entries written or a negative error. */
+int sbb_plan_partition(sbb_plan_t plan, int *h_row, int *h_nnz, int cap);
+int sbb_plan_destroy(sbb_plan_t plan);
+
+const char *sbb_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBB_SPMV_H */

@@ -1,0 +1,81 @@
+// common.cuh — device helpers shared by the SpMV kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sbb {
+
+// Streaming (read-once) loads: evict-first, no L1 allocation, so the col/val
+// streams do not push x out of L2.
+__device__ __forceinline__ int ld_stream(const int *p) { return __ldcs(p); }
+__device__ __forceinline__ int4 ld_stream(const int4 *p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ double2 ld_stream(const double2 *p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ float4 ld_stream(const float4 *p) { return __ldcs(p); }
+
+// x is gathered through the read-only path and kept in L2.
+template <typename T>
+__device__ __forceinline__ T ld_x(const T *p) { return __ldg(p); }
+
+// Column check: out-of-range indices read nothing, contribute 0 and raise the
+// status bit (the host turns it into an error code).
+template <typename T>
+__device__ __forceinline__ T gather_x(const T *x, int c, int n, unsigned &bad)
+{
+    if ((unsigned)c < (unsigned)n) return ld_x(x + c);
+    bad = 1u;
+    return T(0);
+}
+
+// Per-value products for the two storage forms.
+//   FP64: the product itself.
+//   FP32: (p, e) with p = fl(v*x) and e its exact rounding error (fmaf), the
+//         input to the compensated row-segment sum.
+struct ProdF64 {
+    using V = double;
+    using P = double;
+    __device__ __forceinline__ static P make(double v, double xv) { return v * xv; }
+};
+struct ProdF32 {
+    using V = float;
+    using P = float2;
+    __device__ __forceinline__ static P make(float v, float xv)
+    {
+        float p = __fmul_rn(v, xv);
+        float e = __fmaf_rn(v, xv, -p);
+        return make_float2(p, e);
+    }
+};
+
+// Running row-segment sums.  FP64: plain sum.  FP32: Knuth TwoSum with the
+// product errors folded into the compensation term; the segment value is
+// taken to FP64 as s + c.
+struct AccF64 {
+    double s;
+    __device__ __forceinline__ void zero() { s = 0.0; }
+    __device__ __forceinline__ void add(double p) { s += p; }
+    __device__ __forceinline__ double get() const { return s; }
+};
+struct AccF32 {
+    float s, c;
+    __device__ __forceinline__ void zero() { s = 0.f; c = 0.f; }
+    __device__ __forceinline__ void add(float2 p)
+    {
+        float t = __fadd_rn(s, p.x);
+        float bb = __fsub_rn(t, s);
+        float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(p.x, bb));
+        s = t;
+        c = __fadd_rn(c, __fadd_rn(e, p.y));
+    }
+    __device__ __forceinline__ double get() const { return (double)s + (double)c; }
+};
+
+// y update with the cuSPARSE convention: y is not read when beta == 0.
+__device__ __forceinline__ double axpby(double alpha, double sum, double beta,
+                                        const double *yp)
+{
+    return beta == 0.0 ? alpha * sum : alpha * sum + beta * *yp;
+}
+
+}  // namespace sbb

@@ -1,0 +1,101 @@
+// k_vector.cu — K1: vector CSR SpMV, V lanes per row (V = 2..32).
+//
+// Replaces cusparseDcsrmv (SparseBLAS/src/dspmv_mgpu_v1.cu:200-204,
+// src/dspmv_mgpu_baseline.cu:163-167).  A group of V lanes owns one row, reads
+// its col/val with coalesced streaming loads (V consecutive nnz per step),
+// gathers x through the read-only path and reduces with warp shuffles
+// (xor butterfly: the order is fixed for a given V).  Good for regular
+// matrices whose row lengths are close to V; long rows serialise on one group.
+#include "../sbb_internal.h"
+#include "common.cuh"
+
+namespace sbb {
+
+namespace {
+
+constexpr int VT = 256;  // threads per CTA
+
+template <typename PT, typename ACC, int V>
+__global__ void __launch_bounds__(VT)
+vector_kernel(int m, int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+              const typename PT::V *__restrict__ val, const typename PT::V *__restrict__ x,
+              double *__restrict__ y, double alpha, double beta, unsigned *status)
+{
+    const int lane = threadIdx.x & (V - 1);
+    const int group = (blockIdx.x * VT + threadIdx.x) / V;
+    const int groups = gridDim.x * (VT / V);
+    unsigned bad = 0;
+    // The trip count is uniform across the warp (all its groups step together)
+    // so the full-mask shuffles below always see all 32 lanes.
+    const int warp_first = group - ((threadIdx.x & 31) / V);
+    for (int base = warp_first; base < m; base += groups) {
+        const int row = base + (group - warp_first);
+        const bool active = row < m;
+        int lo = 0, hi = 0;
+        if (active) {
+            lo = __ldg(rowptr + row);
+            hi = __ldg(rowptr + row + 1);
+        }
+        ACC acc;
+        acc.zero();
+        int k = lo + lane;
+        // two independent loads in flight per lane
+        for (; k + V < hi; k += 2 * V) {
+            int c0 = ld_stream(col + k), c1 = ld_stream(col + k + V);
+            auto v0 = ld_stream(val + k), v1 = ld_stream(val + k + V);
+            auto x0 = gather_x(x, c0, n, bad), x1 = gather_x(x, c1, n, bad);
+            acc.add(PT::make(v0, x0));
+            acc.add(PT::make(v1, x1));
+        }
+        if (k < hi) acc.add(PT::make(ld_stream(val + k), gather_x(x, ld_stream(col + k), n, bad)));
+        double sum = acc.get();
+#pragma unroll
+        for (int o = V / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, V);
+        if (active && lane == 0) {
+            double *yp = y + row;
+            __stcs(yp, axpby(alpha, sum, beta, yp));
+        }
+    }
+    if (bad) atomicOr(status, ST_BAD_COL);
+}
+
+template <typename PT, typename ACC>
+void launch_vector_t(const CsrView &A, int V, double alpha, const typename PT::V *x,
+                     double beta, double *y, unsigned *status, cudaStream_t s)
+{
+    if (A.m <= 0) return;
+    const auto *val = static_cast<const typename PT::V *>(A.val);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long need = ((long long)A.m * V + VT - 1) / VT;
+    int grid = (int)(need < (long long)sms * 64 ? need : (long long)sms * 64);
+#define SBB_VL(W)                                                                     \
+    case W:                                                                           \
+        vector_kernel<PT, ACC, W><<<grid, VT, 0, s>>>(A.m, A.n, A.rowptr, A.col, val, \
+                                                      x, y, alpha, beta, status);     \
+        break;
+    hook_start(s);
+    switch (V) {
+        SBB_VL(2) SBB_VL(4) SBB_VL(8) SBB_VL(16) SBB_VL(32)
+    default: break;
+    }
+    hook_stop(s);
+#undef SBB_VL
+}
+
+}  // namespace
+
+void launch_vector(const CsrView &A, int V, double alpha, const double *x, double beta,
+                   double *y, unsigned *status, cudaStream_t s)
+{
+    launch_vector_t<ProdF64, AccF64>(A, V, alpha, x, beta, y, status, s);
+}
+
+void launch_vector_f32(const CsrView &A, int V, double alpha, const float *x, double beta,
+                       double *y, unsigned *status, cudaStream_t s)
+{
+    launch_vector_t<ProdF32, AccF32>(A, V, alpha, x, beta, y, status, s);
+}
+
+}  // namespace sbb

@@ -1,0 +1,127 @@
+// sbb_internal.h — shared declarations for libsbb (B200 FP64 CSR SpMV).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "sbb_spmv.h"
+
+namespace sbb {
+
+// ---- error plumbing --------------------------------------------------------
+void set_error(const std::string &msg);
+#define SBB_CUDA(call)                                                        \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) {                                              \
+            ::sbb::set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+            return SBB_ERR_CUDA;                                              \
+        }                                                                     \
+    } while (0)
+
+// Device status word bits, written by kernels instead of trapping.
+enum : unsigned {
+    ST_BAD_ROWPTR = 1u << 0,   // non-monotone row pointer or out of [0, nnz]
+    ST_BAD_COL = 1u << 1,      // column index outside [0, n)
+    ST_BAD_TILE = 1u << 2,     // a merge-path tile with impossible extents
+    ST_BAD_QUEUE = 1u << 3,    // work-queue index past its capacity
+};
+
+// ---- kernel launchers (defined in the .cu files) ---------------------------
+constexpr int kMergeThreads = 256;
+
+struct CsrView {          // rows [0, m) of a CSR matrix; offsets are absolute
+    int m, n;
+    const int *rowptr;    // m+1 entries; rowptr[0] may be non-zero
+    const int *col;
+    const void *val;      // double* (FP64 form) or float* (FP32 form)
+};
+
+// rowptr int64 -> int32 with validation (monotone, within [0, nnz]).
+void launch_rowptr_narrow(const long long *src, int *dst, int m, long long nnz,
+                          unsigned *status, cudaStream_t s);
+void launch_rowptr_check(const int *rp, int m, int nnz, unsigned *status, cudaStream_t s);
+// Row-length statistics: out[0] = max row length, out[1] = #empty rows.
+void launch_row_stats(const int *rowptr, int m, int *out, cudaStream_t s);
+
+// K1: vector CSR, V lanes per row.
+void launch_vector(const CsrView &A, int V, double alpha, const double *x,
+                   double beta, double *y, unsigned *status, cudaStream_t s);
+void launch_vector_f32(const CsrView &A, int V, double alpha, const float *x,
+                       double beta, double *y, unsigned *status, cudaStream_t s);
+
+// K2: merge path.  items = threads*IPT per tile.
+int merge_ipt_supported(int ipt);
+void launch_merge_partition(const int *rowptr, int m, long long items, int tiles,
+                            int *tile_row, int *tile_nnz, cudaStream_t s);
+struct MergeScratch {
+    const int *tile_row, *tile_nnz;   // tiles+1 coordinates
+    int *carry_row;                   // tiles
+    double *carry_val;                // tiles
+    int tiles;
+    unsigned *queue;                  // persistent form: [0] = next tile, [1] = done
+    int persistent_ctas;              // 0 = one CTA per tile
+};
+void launch_merge(const CsrView &A, int ipt, const MergeScratch &S, double alpha,
+                  const double *x, double beta, double *y, unsigned *status,
+                  cudaStream_t s);
+void launch_merge_f32(const CsrView &A, int ipt, const MergeScratch &S,
+                      double alpha, const float *x, double beta, double *y,
+                      unsigned *status, cudaStream_t s);
+int merge_max_ctas_per_sm(int ipt, bool f32);
+// Adds per-tile carries (row, partial) to y in tile order; rows >= m skipped.
+void launch_carry_fixup(int m, const int *carry_row, const double *carry_val, int tiles,
+                        double alpha, double *y, cudaStream_t s);
+
+// Boundary pieces (drop-in): sum of val*x over [lo, hi) per piece.
+void launch_pieces(const long long *lo, const long long *hi, int npieces,
+                   const int *col, const double *val, const double *x, int n,
+                   double *out, unsigned *status, cudaStream_t s);
+
+// Plan object behind sbb_plan_t.
+struct Plan {
+    int m = 0, n = 0, nnz = 0;
+    const int *rowptr = nullptr, *col = nullptr;
+    const void *val = nullptr;
+    bool f32 = false;
+    int kernel = 0;          // resolved SBB_KERNEL_*
+    int vector_width = 0;    // K1
+    int ipt = 0;             // K2
+    int persistent = 0;      // K2 persistent CTAs per SM (0 = off)
+    int tile_sigma = 0;      // K3
+    int max_row = 0, empty_rows = 0;
+    // device scratch owned by the plan
+    int *tile_row = nullptr, *tile_nnz = nullptr, *carry_row = nullptr;
+    double *carry_val = nullptr;
+    unsigned *queue = nullptr;
+    unsigned *status = nullptr;
+    int tiles = 0, persistent_ctas = 0;
+    void *tiled = nullptr;   // K3 tile plan (k_tiled.cu)
+    size_t scratch_bytes = 0;
+    int device = 0;
+};
+
+int plan_build(Plan *p, const sbb_config *cfg, cudaStream_t s);
+int plan_run(Plan *p, double alpha, const void *x, double beta, double *y,
+             cudaStream_t s);
+void plan_free(Plan *p);
+int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *ipt);
+int plan_launches(const Plan *p);
+// Optional timing hooks (set by sbb_spmv_timed for the calling thread): the
+// launchers record them immediately before / after their main kernel.
+struct TimingHooks {
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+TimingHooks &timing_hooks();
+inline void hook_start(cudaStream_t s)
+{
+    if (timing_hooks().start) cudaEventRecord(timing_hooks().start, s);
+}
+inline void hook_stop(cudaStream_t s)
+{
+    if (timing_hooks().stop) cudaEventRecord(timing_hooks().stop, s);
+}
+
+}  // namespace sbb

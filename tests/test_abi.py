@@ -1,0 +1,85 @@
+"""CPU: the C-ABI library loads and exports every symbol include/*.h declares.
+
+No compute call is made here (there is no GPU); only the host-only helpers
+(get_row_from_index, get_time) are called.
+"""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+
+from helpers import golden_grfi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w ]*?[\s\*]+([A-Za-z_]\w*)\s*\(", text,
+                             flags=re.M):
+            if m.group(1) not in ("if", "while", "return", "sizeof"):
+                names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    from sbb._lib import LIB_PATH, SIGNATURES
+    lib = C.CDLL(LIB_PATH)
+    names = declared_functions()
+    assert {"spMV_mgpu_baseline", "spMV_mgpu_v1", "spMV_mgpu_v2", "csr5_kernel",
+            "get_row_from_index", "get_time", "get_gpu_availble_mem"} <= names
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    # the Python bindings cover the same set
+    assert names <= set(SIGNATURES) | {n for n in names if n.startswith("sbb_") and hasattr(lib, n)}
+
+
+def test_cxx_linkage_shims_exported():
+    """The reference's header declares C++ linkage; those mangled names exist too."""
+    from sbb._lib import LIB_PATH
+    lib = C.CDLL(LIB_PATH)
+    for mangled in ("_Z18spMV_mgpu_baselineiixPdS_PxPiS_S_S_i",
+                    "_Z12spMV_mgpu_v1iixPdS_PxPiS_S_S_ii",
+                    "_Z12spMV_mgpu_v2iixPdS_PxPiS_S_S_iixi",
+                    "_Z11csr5_kerneliiiPdS_PiS0_S_S_S_",
+                    "_Z18get_row_from_indexiPxx", "_Z8get_timev", "_Z20get_gpu_availble_memi"):
+        assert hasattr(lib, mangled), mangled
+
+
+def test_get_row_from_index_matches_reference_answers():
+    from sbb import api
+    n = 0
+    for m, rp, idx, row in golden_grfi():
+        assert api.get_row_from_index(m, rp, idx) == row
+        n += 1
+    assert n > 500
+
+
+def test_get_time_is_seconds():
+    from sbb import api
+    t0 = api.get_time()
+    t1 = api.get_time()
+    assert 1.5e9 < t0 <= t1 < 1e11
+
+
+def test_bad_arguments_rejected_before_any_device_work():
+    """Argument checks are host-side: they return -1 without touching a GPU."""
+    from sbb import api
+    rp = np.array([0, 1], np.int64)
+    col = np.zeros(1, np.int32)
+    val = np.ones(1)
+    x = np.ones(1)
+    y = np.zeros(1)
+    assert api.spMV_mgpu_v1(1, 1, 1, 1.0, val, rp, col, x, 0.0, y, ngpu=0, kernel=1) == -1
+    assert api.spMV_mgpu_v1(1, 1, 1, 1.0, val, rp, col, x, 0.0, y, ngpu=1, kernel=4) == -1
+    assert api.spMV_mgpu_v2(1, 1, 1, 1.0, val, rp, col, x, 0.0, y, ngpu=1, kernel=1, nb=0,
+                            q=1) == -1
+    assert api.spMV_mgpu_v2(1, 1, 1, 1.0, val, rp, col, x, 0.0, y, ngpu=1, kernel=1, nb=1,
+                            q=0) == -1
+    bad_rp = np.array([0, 2], np.int64)  # rowptr[m] != nnz
+    assert api.spMV_mgpu_baseline(1, 1, 1, 1.0, val, bad_rp, col, x, 0.0, y, ngpu=1) == -1

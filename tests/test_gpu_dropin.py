@@ -1,0 +1,139 @@
+"""GPU: the drop-in entry points against the reference's own outputs.
+
+Golden fixtures hold the reference drivers' results (tests/golden).  The GPU
+sums in a different order than the reference's csrmv, so FP values are
+compared per row within TOL_FP64 of |alpha|*sum|a_ij x_j| + |beta*y_i|
+(the error metric); return codes and which rows are written must match
+exactly.  The GPU count is pinned to 1, so fixtures made with ngpu > 1 are
+compared with the oracle's ngpu = 1 result.  Kernel 3: the reference's CSR5
+drops alpha and beta; this build honours them, so kernel-3 fixtures are
+compared with the reference where alpha = 1, beta = 0 and with the oracle's
+kernel-1 semantics elsewhere.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import TOL_FP64, golden_cases, max_scaled_err, rand_csr
+
+pytestmark = pytest.mark.gpu
+
+CASES = golden_cases()
+
+
+def _scale(c, rowptr=None):
+    rp = c["rowptr"] if rowptr is None else rowptr
+    _, sc = O.spmv_dd(rp, c["col"], c["val"], c["x"], c["alpha"], c["beta"], c["y"])
+    return sc
+
+
+def _call(api, c, kernel=None, ngpu=None):
+    y = c["y"].copy()
+    args = (c["m"], c["n"], c["nnz"], c["alpha"], c["val"], c["rowptr"], c["col"], c["x"],
+            c["beta"], y)
+    ng = c["ngpu"] if ngpu is None else ngpu
+    k = c["kernel"] if kernel is None else kernel
+    if c["version"] == "baseline":
+        rc = api.spMV_mgpu_baseline(*args, ngpu=ng)
+    elif c["version"] == "v1":
+        rc = api.spMV_mgpu_v1(*args, ngpu=ng, kernel=k)
+    else:
+        rc = api.spMV_mgpu_v2(*args, ngpu=ng, kernel=k, nb=c["nb"], q=c["q"])
+    return rc, y
+
+
+def _expected(c):
+    """The reference's result for this call on one GPU with this build's kernel-3 semantics."""
+    if c["ngpu"] == 1 and (c["kernel"] != 3 or (c["alpha"] == 1.0 and c["beta"] == 0.0)):
+        return c["rc"], c["y_ref"]
+    k = 1 if c["kernel"] == 3 else c["kernel"]
+    return O.dropin(c["version"], c["m"], c["n"], c["nnz"], c["alpha"], c["val"], c["rowptr"],
+                    c["col"], c["x"], c["beta"], c["y"], ngpu=1, kernel=k,
+                    nb=c["nb"] or None, q=c["q"])
+
+
+@pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
+def test_dropin_matches_reference(cuda, c):
+    from sbb import api
+    rc_ref, y_ref = _expected(c)
+    rc, y = _call(api, c)
+    assert rc == rc_ref
+    untouched = y_ref == c["y"]
+    # rows the reference leaves alone must be left alone bit for bit
+    assert np.array_equal(y[untouched & (y_ref == c["y"])], c["y"][untouched])
+    err = max_scaled_err(y, y_ref, _scale(c))
+    assert err <= TOL_FP64, err
+
+
+@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("version", ["v1", "v2"])
+def test_dropin_random_with_empty_rows(cuda, kernel, version):
+    from sbb import api
+    for seed in range(4):
+        m, n = 3000 + 17 * seed, 2500
+        rp, col, val, x, y = rand_csr(100 + seed, m, n, 0, 40, p_empty=0.25,
+                                      long_rows=[(5, 2400), (m - 3, 2000)])
+        nnz = int(rp[-1])
+        alpha, beta = 0.8, (0.0 if seed % 2 else -0.6)
+        nb = max(1, nnz // (1 + 3 * seed)) if version == "v2" else None
+        rc_ref, y_ref = O.dropin(version, m, n, nnz, alpha, val, rp, col, x, beta, y, ngpu=1,
+                                 kernel=1 if kernel == 3 else kernel, nb=nb, q=2)
+        yy = y.copy()
+        if version == "v1":
+            rc = api.spMV_mgpu_v1(m, n, nnz, alpha, val, rp, col, x, beta, yy, ngpu=4,
+                                  kernel=kernel)
+        else:
+            rc = api.spMV_mgpu_v2(m, n, nnz, alpha, val, rp, col, x, beta, yy, ngpu=2,
+                                  kernel=kernel, nb=nb, q=2)
+        assert rc == rc_ref == 0
+        _, sc = O.spmv_dd(rp, col, val, x, alpha, beta, y)
+        assert max_scaled_err(yy, y_ref, sc) <= TOL_FP64
+
+
+def test_dropin_rejects_bad_columns(cuda):
+    from sbb import api
+    rp, col, val, x, y = rand_csr(1, 50, 40, 1, 5)
+    col = col.copy()
+    col[7] = 40  # == n: out of range
+    yy = y.copy()
+    rc = api.spMV_mgpu_v1(50, 40, int(rp[-1]), 1.0, val, rp, col, x, 0.0, yy, ngpu=1, kernel=2)
+    assert rc == -1
+
+
+def test_dropin_rejects_non_monotone_rowptr(cuda):
+    from sbb import api
+    rp, col, val, x, y = rand_csr(2, 50, 40, 1, 5)
+    rp = rp.copy()
+    rp[10], rp[11] = rp[11], rp[10]
+    if rp[10] == rp[11]:
+        rp[10] += 1
+    yy = y.copy()
+    rc = api.spMV_mgpu_v1(50, 40, int(rp[-1]), 1.0, val, rp, col, x, 0.0, yy, ngpu=1, kernel=1)
+    assert rc == -1
+    assert np.array_equal(yy, y)
+
+
+def test_dropin_tiny_and_empty(cuda):
+    from sbb import api
+    # one row, one nnz
+    rp = np.array([0, 1], np.int64)
+    col = np.array([0], np.int32)
+    val = np.array([2.0])
+    x = np.array([3.0])
+    y = np.array([1.0])
+    for k in (1, 2, 3):
+        yy = y.copy()
+        assert api.spMV_mgpu_v1(1, 1, 1, 1.0, val, rp, col, x, 0.5, yy, ngpu=1, kernel=k) == 0
+        assert yy[0] == 6.5
+    # nnz == 0, m == 1: the single row gets beta*y
+    rp0 = np.zeros(2, np.int64)
+    yy = np.array([4.0])
+    assert api.spMV_mgpu_v1(1, 1, 0, 1.0, np.zeros(1), rp0, np.zeros(1, np.int32), x, 0.5, yy,
+                            ngpu=1, kernel=1) == 0
+    assert yy[0] == 2.0
+    # nnz == 0, m >= 2: the partition covers no row (reference: no row written / abort)
+    rp0 = np.zeros(6, np.int64)
+    yy = np.arange(5, dtype=np.float64)
+    assert api.spMV_mgpu_v1(5, 1, 0, 1.0, np.zeros(1), rp0, np.zeros(1, np.int32), x, 0.5, yy,
+                            ngpu=1, kernel=2) == 0
+    assert np.array_equal(yy, np.arange(5, dtype=np.float64))

@@ -1,0 +1,142 @@
+"""GPU: the device API's kernels against the accurate (double-double) oracle.
+
+Error metric per row: |y - y_ref| / (|alpha|*sum_j |a_ij x_j| + |beta*y_i|)
+<= TOL_FP64 (1e-12) for the FP64 kernels.  Integer work (the merge-path
+partition) is compared bit for bit.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import TOL_FP64, max_scaled_err, rand_csr
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = [dict(kernel="vector", vector_width=v) for v in (2, 4, 8, 16, 32)] + \
+          [dict(kernel="merge", items_per_thread=i) for i in (4, 6, 8, 12, 16)] + \
+          [dict(kernel="merge", items_per_thread=8, persistent=p) for p in (1, 2, 4)] + \
+          [dict(kernel="tiled"), dict(kernel="tiled", tile_sigma=4), dict(kernel="tiled", tile_sigma=16),
+           dict(kernel="auto")]
+
+
+def to_dev(rp, col, val, x, y, f32=False):
+    import torch
+    d = torch.device("cuda:0")
+    vt = torch.float32 if f32 else torch.float64
+    return (torch.from_numpy(rp.astype(np.int32)).to(d), torch.from_numpy(col).to(d),
+            torch.from_numpy(val).to(d, vt), torch.from_numpy(x).to(d, vt),
+            torch.from_numpy(y).to(d))
+
+
+def run_plan(rp, col, val, x, y, n, alpha, beta, cfg, reps=1):
+    import torch
+    from sbb.device import Plan
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    P = Plan(drp, dcol, dval, n, **cfg)
+    outs = []
+    for _ in range(reps):
+        yy = dy.clone()
+        P.spmv(dx, yy, alpha, beta)
+        torch.cuda.synchronize()
+        outs.append(yy.cpu().numpy())
+    P.check()
+    info = P.info()
+    P.close()
+    return outs, info
+
+
+MATS = {
+    "uniform": lambda: rand_csr(1, 5000, 4000, 0, 30),
+    "empty_rows": lambda: rand_csr(2, 4000, 3000, 0, 12, p_empty=0.6),
+    "long_rows": lambda: rand_csr(3, 2000, 200000, 0, 8,
+                                  long_rows=[(0, 150000), (999, 70000), (1999, 9000)]),
+    "one_row": lambda: rand_csr(4, 1, 50000, 40000, 40000),
+    "wide": lambda: rand_csr(5, 300, 100000, 100, 2000),
+    "tall": lambda: rand_csr(6, 100000, 500, 0, 3),
+    "all_empty": lambda: rand_csr(7, 777, 100, 0, 0),
+}
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=lambda c: "-".join(f"{v}" for v in c.values()))
+@pytest.mark.parametrize("mat", list(MATS))
+def test_kernel_matches_oracle(cuda, cfg, mat):
+    rp, col, val, x, y = MATS[mat]()
+    n = len(x)
+    for alpha, beta in ((1.0, 0.0), (-0.7, 0.3), (0.0, 2.0)):
+        y_ref, sc = O.spmv_dd(rp, col, val, x, alpha, beta, y)
+        (out,), _ = run_plan(rp, col, val, x, y, n, alpha, beta, cfg)
+        assert max_scaled_err(out, y_ref, sc) <= TOL_FP64, (alpha, beta)
+
+
+@pytest.mark.parametrize("ipt", [4, 8, 16])
+@pytest.mark.parametrize("mat", ["uniform", "empty_rows", "long_rows", "tall"])
+def test_merge_partition_bit_exact(cuda, ipt, mat):
+    import torch
+    from sbb.device import Plan
+    rp, col, val, x, y = MATS[mat]()
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    P = Plan(drp, dcol, dval, len(x), kernel="merge", items_per_thread=ipt)
+    rows, nzs = P.partition()
+    P.close()
+    ref_rows, ref_nzs = O.merge_path_split(rp.astype(np.int32), 256 * ipt, len(rows) - 1)
+    assert np.array_equal(rows, ref_rows) and np.array_equal(nzs, ref_nzs)
+
+
+@pytest.mark.parametrize("cfg", [dict(kernel="merge", items_per_thread=8),
+                                 dict(kernel="merge", items_per_thread=8, persistent=2),
+                                 dict(kernel="vector", vector_width=8), dict(kernel="tiled")])
+def test_repeat_runs_bit_identical(cuda, cfg):
+    rp, col, val, x, y = MATS["long_rows"]()
+    outs, _ = run_plan(rp, col, val, x, y, len(x), 1.3, 0.4, cfg, reps=3)
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+
+
+def test_bad_column_is_flagged_not_faulted(cuda):
+    import torch
+    from sbb.device import Plan, SbbError
+    rp, col, val, x, y = MATS["uniform"]()
+    col = col.copy()
+    col[123] = len(x) + 5
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    P = Plan(drp, dcol, dval, len(x), kernel="merge")
+    P.spmv(dx, dy)
+    with pytest.raises(SbbError):
+        P.check()
+    P.close()
+
+
+def test_bad_rowptr_rejected_at_plan(cuda):
+    from sbb.device import Plan, SbbError
+    rp, col, val, x, y = MATS["uniform"]()
+    rp = rp.copy()
+    rp[100] = rp[101] + 1
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    with pytest.raises(SbbError):
+        Plan(drp, dcol, dval, len(x), kernel="merge")
+
+
+def test_config1_full_parity(cuda):
+    """C1: n = 10,000 power-law matrix, alpha = 1, beta = 0, every kernel."""
+    from sbb import gen
+    A = gen.c1()
+    x = gen.uniform_vec(11, A.n)
+    y = np.zeros(A.m)
+    y_ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x, 1.0, 0.0, y)
+    for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="merge"), dict(kernel="tiled"),
+                dict(kernel="auto")):
+        (out,), _ = run_plan(A.rowptr, A.col, A.val, x, y, A.n, 1.0, 0.0, cfg)
+        assert max_scaled_err(out, y_ref, sc) <= TOL_FP64
+
+
+@pytest.mark.parametrize("which", ["c2", "c3"])
+def test_full_size_parity(cuda, which):
+    """C2 (5.5M rows, 60M nnz, one 1M-nnz row) and C3 at full size vs the oracle."""
+    from sbb import gen
+    A = gen.c2() if which == "c2" else gen.c3()
+    x = gen.uniform_vec(21, A.n)
+    y = gen.uniform_vec(22, A.m)
+    beta = 0.5 if which == "c2" else 0.0
+    y_ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x, 1.0, beta, y)
+    for cfg in (dict(kernel="merge", items_per_thread=8), dict(kernel="tiled"), dict(kernel="auto")):
+        (out,), _ = run_plan(A.rowptr, A.col, A.val, x, y, A.n, 1.0, beta, cfg)
+        assert max_scaled_err(out, y_ref, sc) <= TOL_FP64, cfg
