@@ -229,6 +229,8 @@ def run_sbb(args, ws, rank, local):
     kw = {}
     if args.kernel == "merge":
         kw = dict(items_per_thread=args.ipt, persistent=args.persistent)
+    elif args.kernel == "tiled":
+        kw = dict(tile_sigma=args.sigma)
     P = Plan(rp, col, val, n, kernel=args.kernel, **kw)
     info = P.info()
     launches = lib().sbb_plan_launches(P.h)
@@ -244,6 +246,9 @@ def run_sbb(args, ws, rank, local):
     # timed region: whole steps (value) and the main kernel alone (roofline)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for e in starts + stops:  # torch creates the CUDA event on first record
+        e.record(stream)
+    torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -336,9 +341,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="sbb", choices=["sbb", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
-    ap.add_argument("--kernel", default="merge", choices=["merge", "vector", "tiled", "auto"])
-    ap.add_argument("--ipt", type=int, default=8)
+    ap.add_argument("--kernel", default="tiled", choices=["merge", "vector", "tiled", "auto"])
+    ap.add_argument("--ipt", type=int, default=6)
     ap.add_argument("--persistent", type=int, default=0)
+    ap.add_argument("--sigma", type=int, default=4, help="tiled kernel: nnz per lane (0 = CSR5 rule)")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -36,16 +36,18 @@ int plan_launches(const Plan *p)
 void launch_rowptr_check(const int *rp, int m, int nnz, unsigned *status, cudaStream_t s);
 
 // Default (heuristic) kernel choice, the method without the learned selector:
-// vector CSR when rows are short and even, merge path otherwise.
-int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *ipt)
+// vector CSR when rows are short and even, 32x4 tiles otherwise (the fastest
+// tile shape measured on the irregular benchmark matrices).
+int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *ipt, int *sigma)
 {
     double mean = m > 0 ? (double)nnz / m : 0.0;
     int v = 2;
     while (v < 32 && v < mean) v <<= 1;
     *vector_width = v;
-    *ipt = 8;
+    *ipt = 6;
+    *sigma = 4;
     if (m > 0 && max_row <= 4 * v && max_row <= 128) return SBB_KERNEL_VECTOR;
-    return SBB_KERNEL_MERGE;
+    return SBB_KERNEL_TILED;
 }
 
 static int sm_count(int dev)
@@ -71,24 +73,26 @@ static int dalloc(T **p, size_t count, cudaStream_t s, size_t *acc)
 
 void plan_free_async(Plan *p, cudaStream_t s)
 {
-    void *ptrs[] = {p->tile_row, p->tile_nnz, p->carry_row, p->carry_val, p->queue, p->status};
+    void *ptrs[] = {p->tile_row, p->tile_nnz, p->carry_val, p->queue, p->status};
     for (void *q : ptrs)
         if (q) cudaFreeAsync(q, s);
+    carry_runs_free(&p->runs, s, true);
     extern void tiled_free_async(Plan *, cudaStream_t);
     tiled_free_async(p, s);
-    p->tile_row = p->tile_nnz = p->carry_row = nullptr;
+    p->tile_row = p->tile_nnz = nullptr;
     p->carry_val = nullptr;
     p->queue = p->status = nullptr;
 }
 
 void plan_free(Plan *p)
 {
-    void *ptrs[] = {p->tile_row, p->tile_nnz, p->carry_row, p->carry_val, p->queue, p->status};
+    void *ptrs[] = {p->tile_row, p->tile_nnz, p->carry_val, p->queue, p->status};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    carry_runs_free(&p->runs, 0, false);
     extern void tiled_free(Plan *);
     tiled_free(p);
-    p->tile_row = p->tile_nnz = p->carry_row = nullptr;
+    p->tile_row = p->tile_nnz = nullptr;
     p->carry_val = nullptr;
     p->queue = p->status = nullptr;
 }
@@ -124,23 +128,22 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
     }
     sbb_config c{};
     if (cfg) c = *cfg;
-    int vw = 0, ipt = 0;
+    int vw = 0, ipt = 0, sigma = 0;
     int k = c.kernel;
     if (k == SBB_KERNEL_AUTO) {
-        k = default_kernel_choice(p->m, p->nnz, want_stats ? p->max_row : INT_MAX, &vw, &ipt);
+        k = default_kernel_choice(p->m, p->nnz, want_stats ? p->max_row : INT_MAX, &vw, &ipt, &sigma);
     } else {
-        int dummy_v, dummy_i;
-        default_kernel_choice(p->m, p->nnz, INT_MAX, &dummy_v, &dummy_i);
-        vw = dummy_v;
-        ipt = dummy_i;
+        default_kernel_choice(p->m, p->nnz, INT_MAX, &vw, &ipt, &sigma);
+        sigma = 0;  // an explicit tiled request without a sigma uses the CSR5 rule
     }
     if (c.vector_width) vw = c.vector_width;
     if (c.items_per_thread) ipt = c.items_per_thread;
+    if (c.tile_sigma) sigma = c.tile_sigma;
     p->kernel = k;
     p->vector_width = vw;
     p->ipt = ipt;
     p->persistent = c.persistent;
-    p->tile_sigma = c.tile_sigma;
+    p->tile_sigma = sigma;
     if (k == SBB_KERNEL_VECTOR) {
         if (vw != 2 && vw != 4 && vw != 8 && vw != 16 && vw != 32) {
             set_error("vector_width must be 2, 4, 8, 16 or 32");
@@ -150,10 +153,10 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
     }
     if (k == SBB_KERNEL_MERGE) {
         if (!merge_ipt_supported(ipt)) {
-            set_error("items_per_thread must be 4, 6, 8, 12 or 16");
+            set_error("items_per_thread must be 4, 6, 8 or 12");
             return SBB_ERR_ARG;
         }
-        long long items = (long long)kMergeThreads * ipt;
+        long long items = merge_items_per_tile(ipt);
         long long total = (long long)p->m + p->nnz;
         long long tiles = (total + items - 1) / items;
         if (tiles > INT_MAX - 1) {
@@ -163,24 +166,36 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
         p->tiles = (int)tiles;
         if ((rc = dalloc(&p->tile_row, tiles + 1, s, &p->scratch_bytes))) return rc;
         if ((rc = dalloc(&p->tile_nnz, tiles + 1, s, &p->scratch_bytes))) return rc;
-        if ((rc = dalloc(&p->carry_row, tiles, s, &p->scratch_bytes))) return rc;
         if ((rc = dalloc(&p->carry_val, tiles, s, &p->scratch_bytes))) return rc;
         if ((rc = dalloc(&p->queue, 2, s, &p->scratch_bytes))) return rc;
         SBB_CUDA(cudaMemsetAsync(p->queue, 0, 2 * sizeof(unsigned), s));
-        if (tiles > 0)
+        if (tiles > 0) {
             launch_merge_partition(p->rowptr, p->m, items, p->tiles, p->tile_row, p->tile_nnz, s);
+            if ((rc = carry_runs_build(p->tile_row + 1, p->tiles, p->m, &p->runs, s))) return rc;
+            p->scratch_bytes += p->runs.bytes;
+        }
         if (p->persistent > 0) {
             int occ = merge_max_ctas_per_sm(ipt, p->f32);
             int per_sm = std::min(p->persistent, std::max(occ, 1));
-            p->persistent_ctas = per_sm * sm_count(p->device);
+            p->persistent_ctas = per_sm * sm_count(p->device);  // CTAs of kMergeThreads
         }
         SBB_CUDA(cudaGetLastError());
         return SBB_OK;
     }
     if (k == SBB_KERNEL_TILED) {
         rc = tiled_build(p, s);
-        if (rc == SBB_OK) SBB_CUDA(cudaGetLastError());
-        return rc;
+        if (rc != SBB_OK) return rc;
+        SBB_CUDA(cudaGetLastError());
+        if (validate) {  // the tile copy range-checked every column
+            unsigned st = 0;
+            SBB_CUDA(cudaMemcpyAsync(&st, p->status, sizeof(st), cudaMemcpyDeviceToHost, s));
+            SBB_CUDA(cudaStreamSynchronize(s));
+            if (st & ST_BAD_COL) {
+                set_error("column index out of range [0, n)");
+                return SBB_ERR_INPUT;
+            }
+        }
+        return SBB_OK;
     }
     set_error("unknown kernel id");
     return SBB_ERR_ARG;
@@ -210,7 +225,7 @@ int plan_run(Plan *p, double alpha, const void *x, double beta, double *y, cudaS
                           p->status, s);
         break;
     case SBB_KERNEL_MERGE: {
-        MergeScratch S{p->tile_row, p->tile_nnz, p->carry_row, p->carry_val, p->tiles,
+        MergeScratch S{p->tile_row, p->tile_nnz, p->carry_val, &p->runs, p->tiles,
                        p->queue, p->persistent_ctas};
         if (p->f32)
             launch_merge_f32(A, p->ipt, S, alpha, static_cast<const float *>(x), beta, y,
@@ -335,7 +350,8 @@ int sbb_plan_check(sbb_plan_t plan)
         set_error(std::string("device status ") + std::to_string(st) +
                   ((st & ST_BAD_COL) ? ": column index out of range" : "") +
                   ((st & ST_BAD_TILE) ? ": corrupt tile" : "") +
-                  ((st & ST_BAD_QUEUE) ? ": work queue overflow" : ""));
+                  ((st & ST_BAD_QUEUE) ? ": work queue overflow" : "") +
+                  ((st & ST_TIMEOUT) ? ": a bounded wait on a device copy gave up" : ""));
         return SBB_ERR_INPUT;
     }
     return SBB_OK;

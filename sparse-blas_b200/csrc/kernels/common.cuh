@@ -18,6 +18,44 @@ __device__ __forceinline__ float4 ld_stream(const float4 *p) { return __ldcs(p);
 template <typename T>
 __device__ __forceinline__ T ld_x(const T *p) { return __ldg(p); }
 
+// L2 cache-hint policies: x (gathered many times) is kept, streams are
+// evicted first.
+__device__ __forceinline__ uint64_t l2_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_keep(const double *p, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_keep(const float *p, uint64_t pol)
+{
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+// y read and write with a streaming policy (y is touched once per SpMV).
+__device__ __forceinline__ double ld_y(const double *p, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_y(double *p, double v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+
 // Column check: out-of-range indices read nothing, contribute 0 and raise the
 // status bit (the host turns it into an error code).
 template <typename T>
@@ -76,6 +114,12 @@ __device__ __forceinline__ double axpby(double alpha, double sum, double beta,
                                         const double *yp)
 {
     return beta == 0.0 ? alpha * sum : alpha * sum + beta * *yp;
+}
+// Same, with y read and written under a streaming L2 policy.
+__device__ __forceinline__ void write_y(double *yp, double alpha, double sum, double beta,
+                                        uint64_t pol)
+{
+    st_y(yp, beta == 0.0 ? alpha * sum : alpha * sum + beta * ld_y(yp, pol), pol);
 }
 
 }  // namespace sbb

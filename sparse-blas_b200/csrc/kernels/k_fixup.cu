@@ -1,0 +1,136 @@
+// k_fixup.cu — ordered combination of per-tile carries (K2 and K3).
+//
+// A tiled kernel leaves, for every tile t, the partial sum carry_val[t] of the
+// row still open at the tile's end; the tile where that row ends has already
+// written y = alpha*sum + beta*y for its own part.  Which row each tile
+// carries (carry_row[t], or m for none) depends only on the matrix and the
+// tiling, so it is fixed when the plan is built; so are the runs of
+// consecutive tiles carrying the same row (a long row spans many tiles).
+//
+// Run time: one launch.  Blocks [0, short_blocks) take one tile per thread
+// and add single-tile carries; the remaining blocks take one multi-tile run
+// each and add its carries summed in a fixed order (per-thread strided sums,
+// then a shared-memory tree), so results are bit-reproducible.
+#include "../sbb_internal.h"
+
+namespace sbb {
+
+namespace {
+
+constexpr int FT = 256;
+
+__global__ void runs_mark_kernel(const int *__restrict__ crow, int T, int m,
+                                 int *__restrict__ run_first, int *__restrict__ run_len,
+                                 int *__restrict__ count)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    int r = crow[t];
+    if (r >= m) return;
+    bool head = t == 0 || crow[t - 1] != r;
+    bool multi = t + 1 < T && crow[t + 1] == r;
+    if (!(head && multi)) return;
+    // Run end (equal values are contiguous): exponential probe from t+1, then
+    // bisection between the last index known to carry r and the first known
+    // not to (or T).
+    int lo = t + 1, hi = T, step = 1;
+    for (;;) {
+        int probe = lo + step;
+        if (probe >= T) break;
+        if (crow[probe] != r) {
+            hi = probe;
+            break;
+        }
+        lo = probe;
+        step <<= 1;
+    }
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (crow[mid] == r)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    int j = atomicAdd(count, 1);
+    run_first[j] = t;
+    run_len[j] = lo - t + 1;
+}
+
+__global__ void __launch_bounds__(FT)
+fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cval, int T,
+             const int *__restrict__ run_first, const int *__restrict__ run_len, int short_blocks,
+             double alpha, double *__restrict__ y, unsigned *queue)
+{
+    if (blockIdx.x < short_blocks) {
+        int t = blockIdx.x * FT + threadIdx.x;
+        if (t == 0 && queue != nullptr) queue[0] = 0u;  // rearm a persistent work queue
+        if (t >= T) return;
+        int r = crow[t];
+        if (r >= m) return;
+        if ((t > 0 && crow[t - 1] == r) || (t + 1 < T && crow[t + 1] == r)) return;
+        y[r] += alpha * cval[t];
+        return;
+    }
+    __shared__ double s[FT];
+    const int j = blockIdx.x - short_blocks;
+    const int first = run_first[j], len = run_len[j];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < len; i += FT) acc += cval[first + i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = FT / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) y[crow[first]] += alpha * s[0];
+}
+
+}  // namespace
+
+int carry_runs_build(const int *crow, int T, int m, CarryRuns *R, cudaStream_t s)
+{
+    R->n_runs = 0;
+    R->run_first = R->run_len = nullptr;
+    if (T <= 0) return SBB_OK;
+    int cap = T / 2 + 1;
+    int *count = nullptr;
+    if (cudaMallocAsync((void **)&R->run_first, sizeof(int) * cap, s) != cudaSuccess ||
+        cudaMallocAsync((void **)&R->run_len, sizeof(int) * cap, s) != cudaSuccess ||
+        cudaMallocAsync((void **)&count, sizeof(int), s) != cudaSuccess) {
+        set_error("carry runs: device allocation failed");
+        return SBB_ERR_NOMEM;
+    }
+    R->bytes = 2 * sizeof(int) * (size_t)cap;
+    SBB_CUDA(cudaMemsetAsync(count, 0, sizeof(int), s));
+    runs_mark_kernel<<<(T + FT - 1) / FT, FT, 0, s>>>(crow, T, m, R->run_first, R->run_len, count);
+    int h = 0;
+    SBB_CUDA(cudaMemcpyAsync(&h, count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SBB_CUDA(cudaStreamSynchronize(s));
+    SBB_CUDA(cudaFreeAsync(count, s));
+    R->n_runs = h;
+    return SBB_OK;
+}
+
+void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async)
+{
+    for (int *p : {R->run_first, R->run_len})
+        if (p) {
+            if (async)
+                cudaFreeAsync(p, s);
+            else
+                cudaFree(p);
+        }
+    R->run_first = R->run_len = nullptr;
+    R->n_runs = 0;
+}
+
+void launch_fixup(int m, const int *crow, const double *cval, int T, const CarryRuns &R,
+                  double alpha, double *y, unsigned *queue, cudaStream_t s)
+{
+    if (T <= 0) return;
+    int short_blocks = (T + FT - 1) / FT;
+    fixup_kernel<<<short_blocks + R.n_runs, FT, 0, s>>>(m, crow, cval, T, R.run_first, R.run_len,
+                                                        short_blocks, alpha, y, queue);
+}
+
+}  // namespace sbb

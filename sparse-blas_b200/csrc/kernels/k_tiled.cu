@@ -4,30 +4,35 @@
 // include/anonymouslib_cuda.h, include/detail/cuda/{format,csr5_spmv}_cuda.h)
 // with a design of its own for one B200:
 //
-//   * Tile = 32 lanes x sigma nnz (sigma from the CSR5 rule of
-//     include/anonymouslib_cuda.h:296-313, rounded up to a multiple of 4).
-//     Lane l owns sigma consecutive nnz of the tile.
-//   * The plan keeps a tile-transposed COPY of col/val (the reference
-//     transposes the caller's arrays in place, format_cuda.h:525-744): within
-//     a tile, groups of 4 consecutive nnz of a lane are stored together and the
-//     32 lanes' groups side by side, so every load is a coalesced 128-bit
-//     load (int4 of columns, 2 x double2 / float4 of values).
-//   * Per lane a sigma-bit mask marks which of its nnz start a row
-//     (CSR5's bit-flag descriptor, format_cuda.h:129-360, without the packed
-//     y/scan offsets: the row of each segment comes from a warp scan of the
-//     masks' popcounts instead).
-//   * One warp per tile: each lane sums its segments; rows that end inside the
-//     lane are written at once; a warp segmented scan (reset at lanes that
-//     start a row) joins segments across lanes; the row still open at the tile
-//     end becomes the tile's carry (CSR5's calibrator, csr5_spmv_cuda.h:313-382)
-//     added by the same ordered fix-up as the merge-path kernel - no atomics,
-//     so results are bit-reproducible.
-//   * Empty rows (CSR5's descriptor-offset table, format_cuda.h:362-523) are
-//     handled by a compact list of non-empty rows (segment -> row) and a list
-//     of empty rows that get y = beta*y.
+//   * Tile = 32 lanes x sigma nnz; lane l owns sigma consecutive nnz.  sigma
+//     follows the CSR5 rule (include/anonymouslib_cuda.h:296-313) rounded up
+//     to a power of two in {4, 8, 16, 32}.
+//   * The plan keeps a COPY of the matrix as one blob per tile (the reference
+//     transposes the caller's arrays in place, format_cuda.h:525-744):
+//         [int cols[TILE] | V vals[TILE] | uint32 row-start bitmap[sigma]]
+//     Inside a tile, nnz go in groups of 4 per lane, laid out so every
+//     shared-memory read is 16 contiguous bytes per lane (no bank conflicts).
+//   * One bit per nnz marks row starts (CSR5's bit-flag descriptor,
+//     format_cuda.h:129-360, without the packed y/scan offsets: the row of
+//     each segment comes from a warp scan of the lanes' popcounts).
+//   * Persistent warps take tiles round-robin.  Each warp double-buffers tiles
+//     in shared memory with one TMA bulk copy per tile (cp.async.bulk +
+//     mbarrier, evict-first so x stays in L2; every wait is bounded).  All x
+//     gathers of a lane are issued before any is used.
+//   * Rows ending inside a lane are written at once; a warp segmented scan
+//     (reset at lanes that start a row) joins segments across lanes; the row
+//     open at the tile end is the tile's carry (CSR5's calibrator,
+//     csr5_spmv_cuda.h:313-382) added afterwards in a fixed order
+//     (k_fixup.cu) - no atomics, bit-reproducible.
+//   * Empty rows (CSR5's descriptor-offset table, format_cuda.h:362-523): a
+//     compact list of non-empty rows maps segments to rows, and a list of
+//     empty rows gets y = beta*y.
 //   * Unlike the reference, alpha and beta are applied (csr5_spmv_cuda.h:22
-//     and anonymouslib_cuda.h:281 drop them) and the last partial tile needs no
-//     separate CSR-vector pass (csr5_spmv_cuda.h:384-419): it is padded.
+//     and anonymouslib_cuda.h:281 drop them); the last partial tile is padded
+//     instead of taking a CSR-vector pass (csr5_spmv_cuda.h:384-419).
+#include <stdint.h>
+#include <stdlib.h>
+
 #include <cub/cub.cuh>
 
 #include "../sbb_internal.h"
@@ -37,48 +42,80 @@ namespace sbb {
 
 namespace {
 
-constexpr int TW = 4;  // warps (tiles) per CTA
+constexpr int TW = 4;  // warps per CTA
 
 struct TiledPlan {
     int sigma = 0, tiles = 0;
-    int *col_t = nullptr;
-    void *val_t = nullptr;
-    unsigned *bits = nullptr;     // tiles*32 masks
-    int *tile_seg = nullptr;      // tiles: segment rank of the row holding the tile's first nnz
-    int *ne = nullptr;            // non-empty rows (segment rank -> row), null if none empty
+    size_t tile_bytes = 0;        // one tile blob
+    unsigned char *blob = nullptr;
+    int *tile_seg = nullptr;      // segment rank of the row holding each tile's first nnz
+    int *ne = nullptr;            // non-empty rows (segment rank -> row); null if none empty
     int *empty = nullptr;         // empty rows
     int n_empty = 0;
-    int *carry_row = nullptr;
+    int *carry_row = nullptr;     // static: row carried out of each tile, m if none
     double *carry_val = nullptr;
+    CarryRuns runs;
 };
 
-__global__ void transpose_kernel(const int *__restrict__ rp, const int *__restrict__ col,
-                                 const void *__restrict__ val, int vbytes, long long nnz,
-                                 int sigma, long long total, int *__restrict__ col_t,
-                                 void *__restrict__ val_t)
+__host__ __device__ constexpr size_t tile_bytes_of(int sigma, int vbytes)
 {
-    const long long TILE = 32LL * sigma;
-    const long long first = rp[0];  // the view's nnz start at rowptr[0]
-    for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < total;
-         o += (long long)gridDim.x * blockDim.x) {
-        long long t = o / TILE, q = o % TILE;
-        long long g = q / 128, w = q % 128;  // group of 4 steps, then lane*4 + j
-        long long lane = w / 4, j = w % 4;
-        long long k = t * TILE + lane * sigma + g * 4 + j;  // original nnz index
-        bool in = k < nnz;
-        col_t[o] = in ? col[first + k] : 0;
-        if (vbytes == 8)
-            static_cast<double *>(val_t)[o] = in ? static_cast<const double *>(val)[first + k] : 0.0;
-        else
-            static_cast<float *>(val_t)[o] = in ? static_cast<const float *>(val)[first + k] : 0.f;
-    }
+    return (size_t)32 * sigma * (4 + vbytes) + 4 * (size_t)sigma;
+}
+// Per-warp staging of a tile's row sums: up to 32*sigma + 1 segments (only
+// tiles of sigma >= 8 stage them).
+__host__ __device__ constexpr size_t sum_bytes_of(int sigma)
+{
+    return sigma < 8 ? 0 : ((size_t)(32 * sigma + 1) * 8 + 127) / 128 * 128;
 }
 
-// Row-start bits, non-empty flags.
-__global__ void starts_kernel(const int *__restrict__ rp, int m, int sigma,
-                              unsigned *__restrict__ bits, int *__restrict__ nonempty)
+// Slot of nnz (lane, j) of group g inside a tile, for columns / FP32 values
+// and for FP64 values.
+__device__ __forceinline__ long long slot4(int g, int lane, int j) { return g * 128 + lane * 4 + j; }
+__device__ __forceinline__ long long slot2(int g, int lane, int j)
+{
+    return g * 128 + (j >> 1) * 64 + lane * 2 + (j & 1);
+}
+
+__global__ void blob_fill_kernel(const int *__restrict__ rp, const int *__restrict__ col,
+                                 const void *__restrict__ val, int vbytes, long long nnz, int n,
+                                 int sigma, int tiles, unsigned char *__restrict__ blob,
+                                 unsigned *status)
+{
+    bool bad = false;
+    const long long TILE = 32LL * sigma;
+    const size_t TB = tile_bytes_of(sigma, vbytes);
+    const long long first = rp[0];  // the view's nnz start at rowptr[0]
+    const long long total = (long long)tiles * TILE;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        // e enumerates (tile, lane, group, j) in original nnz order
+        long long t = e / TILE, q = e % TILE;
+        int lane = (int)(q / sigma), s = (int)(q % sigma), g = s >> 2, j = s & 3;
+        bool in = e < nnz;
+        unsigned char *tb = blob + (size_t)t * TB;
+        int c = in ? col[first + e] : 0;
+        if ((unsigned)c >= (unsigned)n) {  // checked once here: the kernel trusts the copy
+            bad |= in;
+            c = 0;
+        }
+        reinterpret_cast<int *>(tb)[slot4(g, lane, j)] = c;
+        if (vbytes == 8)
+            reinterpret_cast<double *>(tb + TILE * 4)[slot2(g, lane, j)] =
+                in ? static_cast<const double *>(val)[first + e] : 0.0;
+        else
+            reinterpret_cast<float *>(tb + TILE * 4)[slot4(g, lane, j)] =
+                in ? static_cast<const float *>(val)[first + e] : 0.f;
+    }
+    if (bad) atomicOr(status, ST_BAD_COL);
+}
+
+// Row-start bits (one per nnz, original order within the tile) and
+// non-empty flags.
+__global__ void starts_kernel(const int *__restrict__ rp, int m, int sigma, int vbytes,
+                              unsigned char *__restrict__ blob, int *__restrict__ nonempty)
 {
     const long long TILE = 32LL * sigma;
+    const size_t TB = tile_bytes_of(sigma, vbytes);
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < m;
          r += (long long)gridDim.x * blockDim.x) {
         int lo = rp[r], hi = rp[r + 1];
@@ -87,7 +124,8 @@ __global__ void starts_kernel(const int *__restrict__ rp, int m, int sigma,
         if (ne) {
             long long k = lo - rp[0];
             long long t = k / TILE, q = k % TILE;
-            atomicOr(bits + t * 32 + q / sigma, 1u << (q % sigma));
+            unsigned *bits = reinterpret_cast<unsigned *>(blob + (size_t)t * TB + TILE * (4 + vbytes));
+            atomicOr(bits + q / 32, 1u << (q % 32));
         }
     }
 }
@@ -107,12 +145,14 @@ __global__ void compact_kernel(const int *__restrict__ flag, const int *__restri
 // Segment rank of the row owning the first nnz of each tile: the last row r
 // with rp[r] <= k (that row is non-empty), mapped through the non-empty rank.
 __global__ void tile_seg_kernel(const int *__restrict__ rp, int m, int sigma, int tiles,
-                                const int *__restrict__ rank, int *__restrict__ tile_seg)
+                                const int *__restrict__ rank, int nonempty,
+                                int *__restrict__ tile_seg)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == tiles) tile_seg[t] = nonempty;  // sentinel: one past the last segment
     if (t >= tiles) return;
     long long k = (long long)rp[0] + (long long)t * 32 * sigma;
-    int lo = 0, hi = m;  // find last r in [0, m) with rp[r] <= k
+    int lo = 0, hi = m;  // last r in [0, m) with rp[r] <= k
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
         if (rp[mid] <= k)
@@ -121,6 +161,30 @@ __global__ void tile_seg_kernel(const int *__restrict__ rp, int m, int sigma, in
             hi = mid - 1;
     }
     tile_seg[t] = rank ? rank[lo] : lo;
+}
+
+__device__ __forceinline__ unsigned first_bit_of_tile(const unsigned char *blob, size_t TB,
+                                                      long long TILE, int vbytes, int t)
+{
+    return *reinterpret_cast<const unsigned *>(blob + (size_t)t * TB + TILE * (4 + vbytes)) & 1u;
+}
+
+// Row carried out of tile t: the row holding its last nnz, when that row goes
+// on into tile t+1 (whose first nnz then starts no row); m otherwise.
+__global__ void carry_rows_kernel(const unsigned char *__restrict__ blob, int sigma, int vbytes,
+                                  const int *__restrict__ tile_seg, const int *__restrict__ ne,
+                                  int tiles, int m, int *__restrict__ carry_row)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tiles) return;
+    const long long TILE = 32LL * sigma;
+    const size_t TB = tile_bytes_of(sigma, vbytes);
+    int r = m;
+    if (t + 1 < tiles && !first_bit_of_tile(blob, TB, TILE, vbytes, t + 1)) {
+        int seg = tile_seg[t + 1];
+        r = ne ? ne[seg] : seg;
+    }
+    carry_row[t] = r;
 }
 
 __global__ void empty_rows_kernel(const int *__restrict__ empty, int n_empty, double beta,
@@ -132,36 +196,126 @@ __global__ void empty_rows_kernel(const int *__restrict__ empty, int n_empty, do
     }
 }
 
-template <typename PT>
-__device__ __forceinline__ void load4(const int *col_t, const typename PT::V *val_t, long long o,
-                                      int4 &c, typename PT::V (&v)[4])
+// ---- TMA (1-D bulk async copy) helpers ------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
-    c = ld_stream(reinterpret_cast<const int4 *>(col_t + o));
-    if constexpr (sizeof(typename PT::V) == 8) {
-        double2 a = ld_stream(reinterpret_cast<const double2 *>(val_t + o));
-        double2 b = ld_stream(reinterpret_cast<const double2 *>(val_t + o + 2));
-        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-    } else {
-        float4 a = ld_stream(reinterpret_cast<const float4 *>(val_t + o));
-        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ uint64_t evict_first_policy()
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// pol == 0: default L2 policy; otherwise an L2 cache-hint policy.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar,
+                                         uint64_t pol)
+{
+    if (pol)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+            " [%0], [%1], %2, [%3], %4;" ::"r"(dst),
+            "l"(src), "r"(bytes), "r"(bar), "l"(pol)
+            : "memory");
+    else
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+            " [%0], [%1], %2, [%3];" ::"r"(dst),
+            "l"(src), "r"(bytes), "r"(bar)
+            : "memory");
+}
+// Bounded wait for the phase with the given parity; false if it never came
+// (the caller raises ST_TIMEOUT and stops instead of spinning for ever).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// One tile from shared memory.
+// Columns in the blob were range-checked when the plan copied them, so x is
+// gathered without a per-element check; the final tile masks its padding.
+template <typename PT, int SIGMA>
+__device__ __forceinline__ void tile_gather(int t, int tiles, long long nnz, const unsigned char *tb,
+                                            const typename PT::V *__restrict__ x, uint64_t keep,
+                                            typename PT::V (&xv)[SIGMA])
+{
+    using V = typename PT::V;
+    constexpr int TILE = 32 * SIGMA;
+    const int lane = threadIdx.x & 31;
+    const int *s_col = reinterpret_cast<const int *>(tb);
+    const long long base = (long long)t * TILE;
+    const bool last = t == tiles - 1;
+#pragma unroll
+    for (int g = 0; g < SIGMA / 4; ++g) {
+        const int4 c = *reinterpret_cast<const int4 *>(s_col + g * 128 + lane * 4);
+        const int cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (last)
+                xv[g * 4 + j] = base + lane * SIGMA + g * 4 + j < nnz ? ld_keep(x + cc[j], keep) : V(0);
+            else
+                xv[g * 4 + j] = ld_keep(x + cc[j], keep);
+        }
     }
 }
 
+// Reduces one tile whose x values are already gathered (xv).  Row sums are
+// staged in the warp's s_sum (index = segment - tseg) and written to y in one
+// coalesced pass at the end, so the divergent per-nnz loop touches no global
+// memory; ya/yb hold y of segments tseg+lane and tseg+32+lane, loaded when
+// the tile started.
 template <typename PT, typename ACC, int SIGMA>
-__global__ void __launch_bounds__(TW * 32)
-tiled_kernel(int m, int n, long long nnz, int tiles, const int *__restrict__ col_t,
-             const typename PT::V *__restrict__ val_t, const unsigned *__restrict__ bits_arr,
-             const int *__restrict__ tile_seg, const int *__restrict__ ne,
-             const typename PT::V *__restrict__ x, double *__restrict__ y, double alpha,
-             double beta, int *__restrict__ carry_row, double *__restrict__ carry_val,
-             unsigned *status)
+__device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned char *tb, int tseg,
+                                            unsigned next_bit0, const int *__restrict__ ne,
+                                            const typename PT::V (&xv)[SIGMA],
+                                            double *__restrict__ y, double alpha, double beta,
+                                            double *__restrict__ carry_val, uint64_t stream,
+                                            double ya, double yb, double *s_sum)
 {
+    using V = typename PT::V;
     constexpr int TILE = 32 * SIGMA;
+    constexpr int G = SIGMA / 4;
     const int lane = threadIdx.x & 31;
-    const int t = blockIdx.x * TW + (threadIdx.x >> 5);
-    if (t >= tiles) return;  // warp-uniform
-    const long long base = (long long)t * TILE;
-    const unsigned bits = __ldg(bits_arr + (long long)t * 32 + lane);
+    const V *s_val = reinterpret_cast<const V *>(tb + TILE * 4);
+    const unsigned *s_bits = reinterpret_cast<const unsigned *>(tb + TILE * (4 + sizeof(V)));
+
+    // this lane's sigma row-start bits
+    unsigned bits;
+    if constexpr (SIGMA == 32)
+        bits = s_bits[lane];
+    else
+        bits = (s_bits[(lane * SIGMA) >> 5] >> ((lane * SIGMA) & 31)) & ((1u << SIGMA) - 1u);
+
+    // 2. segment rows of this lane.  Tiles of sigma >= 8 stage row sums and
+    // write them in one coalesced pass; sigma = 4 tiles (few rows per lane,
+    // tightest register budget) write each row as it completes.
+    constexpr bool kStaged = SIGMA >= 8;
+    auto put = [&](int sg, double sum) {
+        if (kStaged)
+            s_sum[sg - tseg] = sum;
+        else
+            write_y(y + (ne ? __ldg(ne + sg) : sg), alpha, sum, beta, stream);
+    };
     const unsigned b0 = __shfl_sync(0xffffffffu, bits, 0) & 1u;
     const int cnt = __popc(bits);
     int incl = cnt;
@@ -170,23 +324,25 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const int *__restrict__ col
         int u = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += u;
     }
-    const int seg0 = __ldg(tile_seg + t) - (int)b0;
-    const int head_seg = seg0 + incl - cnt;  // segment open before this lane's first nnz
-    auto row_of = [&](int seg) { return ne ? __ldg(ne + seg) : seg; };
+    const int head_seg = tseg - (int)b0 + incl - cnt;  // segment open before this lane's first nnz
 
-    unsigned bad = 0;
-    const bool last = t == tiles - 1;
+    // 3. products and lane-local segmented sums
     ACC acc;
     acc.zero();
     double head = 0.0;
     bool started = false;
     int seg = head_seg;
 #pragma unroll
-    for (int g = 0; g < SIGMA / 4; ++g) {
-        int4 c;
-        typename PT::V v[4];
-        load4<PT>(col_t, val_t, base + g * 128 + lane * 4, c, v);
-        const int cc[4] = {c.x, c.y, c.z, c.w};
+    for (int g = 0; g < G; ++g) {
+        V v[4];
+        if constexpr (sizeof(V) == 8) {
+            double2 a = *reinterpret_cast<const double2 *>(s_val + g * 128 + lane * 2);
+            double2 b = *reinterpret_cast<const double2 *>(s_val + g * 128 + 64 + lane * 2);
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+        } else {
+            float4 a = *reinterpret_cast<const float4 *>(s_val + g * 128 + lane * 4);
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int s = g * 4 + j;
@@ -195,17 +351,16 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const int *__restrict__ col
                     head = acc.get();
                     started = true;
                 } else {  // a whole row inside this lane
-                    double *yp = y + row_of(seg);
-                    *yp = axpby(alpha, acc.get(), beta, yp);
+                    put(seg, acc.get());
                 }
                 acc.zero();
                 ++seg;
             }
-            const bool live = !last || base + lane * SIGMA + s < nnz;
-            if (live) acc.add(PT::make(v[j], gather_x(x, cc[j], n, bad)));
+            acc.add(PT::make(v[j], xv[s]));
         }
     }
-    // Warp segmented scan of lane carries, reset at lanes that start a row.
+
+    // 4. warp segmented scan of lane carries, reset at lanes that start a row
     double cv = acc.get();  // tail (or whole lane when no row starts here)
     unsigned f = started;
 #pragma unroll
@@ -222,24 +377,140 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const int *__restrict__ col
     // The row open when this lane began ends at its first row start.  For
     // lane 0 with a start on its first nnz that row ended with the previous
     // tile, which wrote it.
-    if (started && !(lane == 0 && b0)) {
-        double *yp = y + row_of(head_seg);
-        *yp = axpby(alpha, incoming + head, beta, yp);
-    }
+    if (started && !(lane == 0 && b0)) put(head_seg, incoming + head);
+    const bool closes = last || next_bit0;  // the open row ends with this tile
     if (lane == 31) {
-        const bool closes = last || (__ldg(bits_arr + (long long)(t + 1) * 32) & 1u);
-        const int r = row_of(seg);
         if (closes) {
-            double *yp = y + r;
-            *yp = axpby(alpha, cv, beta, yp);
-            carry_row[t] = m;  // nothing to carry
-            carry_val[t] = 0.0;
+            put(seg, cv);
+            carry_val[t] = 0.0;  // carry_row[t] == m
         } else {
-            carry_row[t] = r;
-            carry_val[t] = cv;
+            carry_val[t] = cv;   // carried into row_of(seg) == carry_row[t]
         }
     }
-    if (bad) atomicOr(status, ST_BAD_COL);
+    if (!kStaged) return;
+    // 5. rows completed here: segments tseg .. tseg+nwrite-1, coalesced
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int nwrite = total + (closes ? 1 : 0) - (int)b0;
+    __syncwarp();
+    for (int i = lane; i < nwrite; i += 32) {
+        double *yp = y + (ne ? __ldg(ne + tseg + i) : tseg + i);
+        double v = alpha * s_sum[i];
+        if (beta != 0.0) v += beta * (i < 32 ? ya : (i < 64 ? yb : ld_y(yp, stream)));
+        st_y(yp, v, stream);
+    }
+    __syncwarp();  // s_sum is reused by the next tile
+}
+
+// CTAs per SM the launch bounds aim at.
+template <int SIGMA> struct TiledShape {
+    static constexpr int MINB = SIGMA <= 4 ? 12 : (SIGMA <= 8 ? 8 : 1);
+};
+
+// Persistent: warp w of the grid takes tiles w, w + W, w + 2W, ... (W = all
+// warps), fixed per launch shape, so results do not depend on timing.  Each
+// warp keeps a ring of NBUF tile blobs in shared memory: lane 0 issues the
+// bulk copy of tile i+NBUF as soon as tile i is reduced.
+template <typename PT, typename ACC, int SIGMA, int NBUF>
+__global__ void __launch_bounds__(TW * 32, TiledShape<SIGMA>::MINB)
+tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__restrict__ blob,
+             const int *__restrict__ tile_seg, const int *__restrict__ ne,
+             const typename PT::V *__restrict__ x, double *__restrict__ y, double alpha,
+             double beta, double *__restrict__ carry_val, unsigned *status, int evict_first)
+{
+    using V = typename PT::V;
+    constexpr int TILE = 32 * SIGMA;
+    constexpr uint32_t TB = (uint32_t)tile_bytes_of(SIGMA, sizeof(V));
+    constexpr uint32_t SB = (uint32_t)sum_bytes_of(SIGMA);
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[TW][NBUF];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *wbuf = smem + (size_t)warp * (NBUF * TB + SB);
+    double *s_sum = reinterpret_cast<double *>(wbuf + NBUF * TB);
+    const uint32_t bar_base = smem_u32(&bars[warp][0]);
+    const int W = gridDim.x * TW;
+    int t = blockIdx.x * TW + warp;
+    (void)m;
+    (void)n;
+
+    uint64_t pol = 0;
+    auto issue = [&](int tt, int b) {  // lane 0 only
+        const uint32_t bar = bar_base + 8 * b;
+        mbar_expect_tx(bar, TB);
+        bulk_g2s(smem_u32(wbuf + b * TB), blob + (size_t)tt * TB, TB, bar, pol);
+    };
+    if (lane == 0) {
+        pol = evict_first ? evict_first_policy() : 0;
+#pragma unroll
+        for (int b = 0; b < NBUF; ++b) mbar_init(bar_base + 8 * b, 1);
+        mbar_fence_init();
+#pragma unroll
+        for (int b = 0; b < NBUF; ++b)
+            if (t + b * W < tiles) issue(t + b * W, b);
+    }
+    __syncwarp();
+
+    auto next_bit0_of = [&](int tt) -> unsigned {
+        return tt + 1 < tiles ? (__ldg(reinterpret_cast<const unsigned *>(
+                                     blob + (size_t)(tt + 1) * TB + TILE * (4 + sizeof(V)))) & 1u)
+                              : 0u;
+    };
+    unsigned timeout = 0;
+    uint32_t phases = 0u;  // bit b: parity of buffer b's next phase
+    const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
+    auto wait_buf = [&](int bb) {
+        bool ok = mbar_wait(bar_base + 8 * bb, (phases >> bb) & 1u);
+        phases ^= 1u << bb;
+        return ok;
+    };
+    int b = 0;
+    int tseg = 0, tseg1 = 0;
+    unsigned nb0 = 0;
+    if (t < tiles) {
+        tseg = __ldg(tile_seg + t);
+        tseg1 = __ldg(tile_seg + t + 1);
+        nb0 = next_bit0_of(t);
+    }
+    for (; t < tiles; t += W) {
+        // y of the segments this tile can write (tile_seg[t] .. tile_seg[t+1]),
+        // loaded now so the write pass does not wait for it
+        double ya = 0.0, yb = 0.0;
+        if (SIGMA >= 8 && beta != 0.0) {
+            const int lim = tseg1 + (t + 1 < tiles ? 1 : 0);
+            if (tseg + lane < lim) ya = ld_y(y + (ne ? __ldg(ne + tseg + lane) : tseg + lane), streaming);
+            if (tseg + 32 + lane < lim)
+                yb = ld_y(y + (ne ? __ldg(ne + tseg + 32 + lane) : tseg + 32 + lane), streaming);
+        }
+        // metadata of the next tile, in flight while this one is reduced
+        const int tn = t + W;
+        int tseg_n = 0, tseg1_n = 0;
+        unsigned nb0_n = 0;
+        if (tn < tiles) {
+            tseg_n = __ldg(tile_seg + tn);
+            tseg1_n = __ldg(tile_seg + tn + 1);
+            nb0_n = next_bit0_of(tn);
+        }
+        if (!wait_buf(b)) {
+            timeout = 1;
+            break;
+        }
+        V xv[SIGMA];
+        tile_gather<PT, SIGMA>(t, tiles, nnz, wbuf + b * TB, x, keep, xv);
+        tile_reduce<PT, ACC, SIGMA>(t, t == tiles - 1, wbuf + b * TB, tseg, nb0, ne, xv, y, alpha,
+                                    beta, carry_val, streaming, ya, yb, s_sum);
+        __syncwarp();  // every lane is done with buffer b before it is refilled
+        if (lane == 0 && t + NBUF * W < tiles) issue(t + NBUF * W, b);
+        b = b + 1 == NBUF ? 0 : b + 1;
+        tseg = tseg_n;
+        tseg1 = tseg1_n;
+        nb0 = nb0_n;
+    }
+    if (timeout) {
+        // let copies still in flight land (bounded) before the warp leaves
+#pragma unroll
+        for (int bb = 0; bb < NBUF; ++bb) mbar_wait(bar_base + 8 * bb, (phases >> bb) & 1u);
+        if (lane == 0) atomicOr(status, ST_TIMEOUT);
+    }
+    (void)status;
 }
 
 int grid_for(long long work, int tpb)
@@ -250,29 +521,70 @@ int grid_for(long long work, int tpb)
     return (int)g;
 }
 
+// Pipeline depth (tile blobs in flight per warp) and the L2 policy of the
+// bulk copies; SBB_TILED_STAGES / SBB_TILED_EVICT_FIRST override the defaults.
+struct TiledTuning {
+    int stages, evict_first;
+};
+static TiledTuning tiled_tuning()
+{
+    TiledTuning t{2, 1};
+    if (const char *e = getenv("SBB_TILED_STAGES")) t.stages = atoi(e);
+    if (const char *e = getenv("SBB_TILED_EVICT_FIRST")) t.evict_first = atoi(e);
+    if (t.stages < 2 || t.stages > 4) t.stages = 2;
+    return t;
+}
+
+template <typename PT, typename ACC, int SIGMA, int NBUF>
+void launch_tiled_n(const TiledPlan &T, int m, int n, long long nnz, double alpha,
+                    const typename PT::V *x, double beta, double *y, unsigned *status,
+                    int evict_first, cudaStream_t s)
+{
+    auto kern = tiled_kernel<PT, ACC, SIGMA, NBUF>;
+    constexpr size_t smem =
+        (size_t)TW * (NBUF * tile_bytes_of(SIGMA, sizeof(typename PT::V)) + sum_bytes_of(SIGMA));
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TW * 32, smem);
+    long long want = (T.tiles + TW - 1) / TW;
+    long long cap = (long long)sms * (occ > 0 ? occ : 1);
+    int grid = (int)(want < cap ? want : cap);
+    hook_start(s);
+    kern<<<grid, TW * 32, smem, s>>>(m, n, nnz, T.tiles, T.blob, T.tile_seg, T.ne, x, y, alpha,
+                                     beta, T.carry_val, status, evict_first);
+    hook_stop(s);
+}
+
+template <typename PT, typename ACC, int SIGMA>
+void launch_tiled_s(const TiledPlan &T, int m, int n, long long nnz, double alpha,
+                    const typename PT::V *x, double beta, double *y, unsigned *status,
+                    cudaStream_t s)
+{
+    const TiledTuning tu = tiled_tuning();
+    if (SIGMA <= 8 && tu.stages == 3)
+        launch_tiled_n<PT, ACC, SIGMA, 3>(T, m, n, nnz, alpha, x, beta, y, status, tu.evict_first, s);
+    else if (SIGMA <= 8 && tu.stages == 4)
+        launch_tiled_n<PT, ACC, SIGMA, 4>(T, m, n, nnz, alpha, x, beta, y, status, tu.evict_first, s);
+    else
+        launch_tiled_n<PT, ACC, SIGMA, 2>(T, m, n, nnz, alpha, x, beta, y, status, tu.evict_first, s);
+}
+
 template <typename PT, typename ACC>
 void launch_tiled_t(const TiledPlan &T, int m, int n, long long nnz, double alpha,
                     const typename PT::V *x, double beta, double *y, unsigned *status,
                     cudaStream_t s)
 {
     if (T.tiles > 0) {
-        const auto *val_t = static_cast<const typename PT::V *>(T.val_t);
-        int grid = (T.tiles + TW - 1) / TW;
-        hook_start(s);
-#define SBB_TL(S)                                                                          \
-    case S:                                                                                \
-        tiled_kernel<PT, ACC, S><<<grid, TW * 32, 0, s>>>(m, n, nnz, T.tiles, T.col_t, val_t, \
-                                                          T.bits, T.tile_seg, T.ne, x, y,  \
-                                                          alpha, beta, T.carry_row,        \
-                                                          T.carry_val, status);            \
-        break;
         switch (T.sigma) {
-            SBB_TL(4) SBB_TL(8) SBB_TL(12) SBB_TL(16) SBB_TL(20) SBB_TL(24) SBB_TL(28) SBB_TL(32)
+        case 4: launch_tiled_s<PT, ACC, 4>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
+        case 8: launch_tiled_s<PT, ACC, 8>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
+        case 16: launch_tiled_s<PT, ACC, 16>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
+        case 32: launch_tiled_s<PT, ACC, 32>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
         default: break;
         }
-#undef SBB_TL
-        hook_stop(s);
-        launch_carry_fixup(m, T.carry_row, T.carry_val, T.tiles, alpha, y, s);
+        launch_fixup(m, T.carry_row, T.carry_val, T.tiles, T.runs, alpha, y, nullptr, s);
     }
     if (T.n_empty > 0)
         empty_rows_kernel<<<grid_for(T.n_empty, 256), 256, 0, s>>>(T.empty, T.n_empty, beta, y);
@@ -281,7 +593,7 @@ void launch_tiled_t(const TiledPlan &T, int m, int n, long long nnz, double alph
 }  // namespace
 
 // CSR5 sigma rule (include/anonymouslib_cuda.h:296-313), then rounded up to a
-// multiple of 4 for the 128-bit tile layout.
+// power of two in {4, 8, 16, 32} so a lane's row-start bits sit in one word.
 int tiled_sigma(int m, long long nnz, int requested)
 {
     int s = requested;
@@ -296,8 +608,9 @@ int tiled_sigma(int m, long long nnz, int requested)
         else
             s = 6;
     }
-    s = ((s + 3) / 4) * 4;
-    return s < 4 ? 4 : (s > 32 ? 32 : s);
+    int p = 4;
+    while (p < s && p < 32) p <<= 1;
+    return p;
 }
 
 int tiled_build(Plan *p, cudaStream_t s)
@@ -306,12 +619,12 @@ int tiled_build(Plan *p, cudaStream_t s)
     p->tiled = T;
     T->sigma = tiled_sigma(p->m, p->nnz, p->tile_sigma);
     p->tile_sigma = T->sigma;
+    const int vbytes = p->f32 ? 4 : 8;
     const long long TILE = 32LL * T->sigma;
     const long long tiles = (p->nnz + TILE - 1) / TILE;
     T->tiles = (int)tiles;
     p->tiles = T->tiles;
-    const long long total = tiles * TILE;
-    const int vbytes = p->f32 ? 4 : 8;
+    T->tile_bytes = tile_bytes_of(T->sigma, vbytes);
     auto al = [&](void **ptr, size_t bytes) {
         bytes = bytes ? bytes : 16;
         p->scratch_bytes += bytes;
@@ -319,9 +632,8 @@ int tiled_build(Plan *p, cudaStream_t s)
     };
     const int m = p->m;
     int *flag = nullptr, *rank = nullptr;
-    bool ok = al((void **)&T->col_t, sizeof(int) * total) && al(&T->val_t, (size_t)vbytes * total) &&
-              al((void **)&T->bits, sizeof(unsigned) * (tiles + 1) * 32) &&
-              al((void **)&T->tile_seg, sizeof(int) * tiles) &&
+    bool ok = al((void **)&T->blob, T->tile_bytes * (size_t)tiles) &&
+              al((void **)&T->tile_seg, sizeof(int) * (tiles + 1)) &&
               al((void **)&T->carry_row, sizeof(int) * tiles) &&
               al((void **)&T->carry_val, sizeof(double) * tiles) &&
               al((void **)&flag, sizeof(int) * (m + 1)) && al((void **)&rank, sizeof(int) * (m + 1));
@@ -329,11 +641,15 @@ int tiled_build(Plan *p, cudaStream_t s)
         set_error("tiled plan: device allocation failed");
         return SBB_ERR_NOMEM;
     }
-    if (total > 0)
-        transpose_kernel<<<grid_for(total, 256), 256, 0, s>>>(p->rowptr, p->col, p->val, vbytes, p->nnz,
-                                                              T->sigma, total, T->col_t, T->val_t);
-    SBB_CUDA(cudaMemsetAsync(T->bits, 0, sizeof(unsigned) * (tiles + 1) * 32, s));
-    if (m > 0) starts_kernel<<<grid_for(m, 256), 256, 0, s>>>(p->rowptr, m, T->sigma, T->bits, flag);
+    if (tiles > 0) {
+        // bitmaps are OR-ed into zeroed words; cols/vals are then written over
+        SBB_CUDA(cudaMemsetAsync(T->blob, 0, T->tile_bytes * (size_t)tiles, s));
+        blob_fill_kernel<<<grid_for(tiles * TILE, 256), 256, 0, s>>>(
+            p->rowptr, p->col, p->val, vbytes, p->nnz, p->n, T->sigma, T->tiles, T->blob,
+            p->status);
+    }
+    if (m > 0)
+        starts_kernel<<<grid_for(m, 256), 256, 0, s>>>(p->rowptr, m, T->sigma, vbytes, T->blob, flag);
     // rank[r] = number of non-empty rows before r (rank[m] = count)
     SBB_CUDA(cudaMemsetAsync(flag + m, 0, sizeof(int), s));
     size_t tmp_bytes = 0;
@@ -351,10 +667,16 @@ int tiled_build(Plan *p, cudaStream_t s)
             return SBB_ERR_NOMEM;
         compact_kernel<<<grid_for(m, 256), 256, 0, s>>>(flag, rank, m, T->ne, T->empty);
     }
-    if (tiles > 0)
-        tile_seg_kernel<<<(T->tiles + 255) / 256, 256, 0, s>>>(p->rowptr, m, T->sigma, T->tiles,
-                                                              T->n_empty > 0 ? rank : nullptr,
-                                                              T->tile_seg);
+    if (tiles > 0) {
+        tile_seg_kernel<<<(T->tiles + 256) / 256, 256, 0, s>>>(
+            p->rowptr, m, T->sigma, T->tiles, T->n_empty > 0 ? rank : nullptr, count,
+            T->tile_seg);
+        carry_rows_kernel<<<(T->tiles + 255) / 256, 256, 0, s>>>(
+            T->blob, T->sigma, vbytes, T->tile_seg, T->ne, T->tiles, m, T->carry_row);
+        int rc = carry_runs_build(T->carry_row, T->tiles, m, &T->runs, s);
+        if (rc) return rc;
+        p->scratch_bytes += T->runs.bytes;
+    }
     SBB_CUDA(cudaFreeAsync(tmp, s));
     SBB_CUDA(cudaFreeAsync(flag, s));
     SBB_CUDA(cudaFreeAsync(rank, s));
@@ -383,8 +705,7 @@ static void tiled_release(Plan *p, cudaStream_t s, bool async)
 {
     auto *T = static_cast<TiledPlan *>(p->tiled);
     if (!T) return;
-    void *ptrs[] = {T->col_t, T->val_t, T->bits, T->tile_seg, T->ne, T->empty, T->carry_row,
-                    T->carry_val};
+    void *ptrs[] = {T->blob, T->tile_seg, T->ne, T->empty, T->carry_row, T->carry_val};
     for (void *q : ptrs)
         if (q) {
             if (async)
@@ -392,11 +713,13 @@ static void tiled_release(Plan *p, cudaStream_t s, bool async)
             else
                 cudaFree(q);
         }
+    carry_runs_free(&T->runs, s, async);
     delete T;
     p->tiled = nullptr;
 }
 
 void tiled_free(Plan *p) { tiled_release(p, 0, false); }
+void tiled_free_async(Plan *p, cudaStream_t s) { tiled_release(p, s, true); }
 
 int tiled_launches(const Plan *p)
 {
@@ -404,6 +727,5 @@ int tiled_launches(const Plan *p)
     if (!T) return 0;
     return (T->tiles > 0 ? 2 : 0) + (T->n_empty > 0 ? 1 : 0);
 }
-void tiled_free_async(Plan *p, cudaStream_t s) { tiled_release(p, s, true); }
 
 }  // namespace sbb

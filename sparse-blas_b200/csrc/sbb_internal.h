@@ -27,6 +27,7 @@ enum : unsigned {
     ST_BAD_COL = 1u << 1,      // column index outside [0, n)
     ST_BAD_TILE = 1u << 2,     // a merge-path tile with impossible extents
     ST_BAD_QUEUE = 1u << 3,    // work-queue index past its capacity
+    ST_TIMEOUT = 1u << 4,      // a bounded wait on a copy gave up
 };
 
 // ---- kernel launchers (defined in the .cu files) ---------------------------
@@ -52,14 +53,29 @@ void launch_vector(const CsrView &A, int V, double alpha, const double *x,
 void launch_vector_f32(const CsrView &A, int V, double alpha, const float *x,
                        double beta, double *y, unsigned *status, cudaStream_t s);
 
-// K2: merge path.  items = threads*IPT per tile.
+// Per-tile carries: carry_row[t] (static per plan; m = nothing carried) and
+// carry_val[t] (written by the tiled kernel).  Runs of >= 2 tiles carrying
+// the same row are listed once at plan time.
+struct CarryRuns {
+    int *run_first = nullptr, *run_len = nullptr;
+    int n_runs = 0;
+    size_t bytes = 0;
+};
+int carry_runs_build(const int *carry_row, int T, int m, CarryRuns *R, cudaStream_t s);
+void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async);
+// Adds the carries to y in a fixed order; also rearms `queue` when non-null.
+void launch_fixup(int m, const int *carry_row, const double *carry_val, int T,
+                  const CarryRuns &R, double alpha, double *y, unsigned *queue, cudaStream_t s);
+
+// K2: merge path.  One warp per segment of 32*IPT merge items.
 int merge_ipt_supported(int ipt);
+long long merge_items_per_tile(int ipt);
 void launch_merge_partition(const int *rowptr, int m, long long items, int tiles,
                             int *tile_row, int *tile_nnz, cudaStream_t s);
 struct MergeScratch {
-    const int *tile_row, *tile_nnz;   // tiles+1 coordinates
-    int *carry_row;                   // tiles
+    const int *tile_row, *tile_nnz;   // tiles+1 coordinates; tile t carries row tile_row[t+1]
     double *carry_val;                // tiles
+    const CarryRuns *runs;
     int tiles;
     unsigned *queue;                  // persistent form: [0] = next tile, [1] = done
     int persistent_ctas;              // 0 = one CTA per tile
@@ -71,9 +87,7 @@ void launch_merge_f32(const CsrView &A, int ipt, const MergeScratch &S,
                       double alpha, const float *x, double beta, double *y,
                       unsigned *status, cudaStream_t s);
 int merge_max_ctas_per_sm(int ipt, bool f32);
-// Adds per-tile carries (row, partial) to y in tile order; rows >= m skipped.
-void launch_carry_fixup(int m, const int *carry_row, const double *carry_val, int tiles,
-                        double alpha, double *y, cudaStream_t s);
+
 
 // Boundary pieces (drop-in): sum of val*x over [lo, hi) per piece.
 void launch_pieces(const long long *lo, const long long *hi, int npieces,
@@ -93,8 +107,9 @@ struct Plan {
     int tile_sigma = 0;      // K3
     int max_row = 0, empty_rows = 0;
     // device scratch owned by the plan
-    int *tile_row = nullptr, *tile_nnz = nullptr, *carry_row = nullptr;
+    int *tile_row = nullptr, *tile_nnz = nullptr;
     double *carry_val = nullptr;
+    CarryRuns runs;
     unsigned *queue = nullptr;
     unsigned *status = nullptr;
     int tiles = 0, persistent_ctas = 0;
@@ -107,7 +122,7 @@ int plan_build(Plan *p, const sbb_config *cfg, cudaStream_t s);
 int plan_run(Plan *p, double alpha, const void *x, double beta, double *y,
              cudaStream_t s);
 void plan_free(Plan *p);
-int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *ipt);
+int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *ipt, int *sigma);
 int plan_launches(const Plan *p);
 // Optional timing hooks (set by sbb_spmv_timed for the calling thread): the
 // launchers record them immediately before / after their main kernel.

@@ -13,7 +13,7 @@ from helpers import TOL_FP64, max_scaled_err, rand_csr
 pytestmark = pytest.mark.gpu
 
 CONFIGS = [dict(kernel="vector", vector_width=v) for v in (2, 4, 8, 16, 32)] + \
-          [dict(kernel="merge", items_per_thread=i) for i in (4, 6, 8, 12, 16)] + \
+          [dict(kernel="merge", items_per_thread=i) for i in (4, 6, 8, 12)] + \
           [dict(kernel="merge", items_per_thread=8, persistent=p) for p in (1, 2, 4)] + \
           [dict(kernel="tiled"), dict(kernel="tiled", tile_sigma=4), dict(kernel="tiled", tile_sigma=16),
            dict(kernel="auto")]
@@ -68,7 +68,7 @@ def test_kernel_matches_oracle(cuda, cfg, mat):
         assert max_scaled_err(out, y_ref, sc) <= TOL_FP64, (alpha, beta)
 
 
-@pytest.mark.parametrize("ipt", [4, 8, 16])
+@pytest.mark.parametrize("ipt", [4, 8, 12])
 @pytest.mark.parametrize("mat", ["uniform", "empty_rows", "long_rows", "tall"])
 def test_merge_partition_bit_exact(cuda, ipt, mat):
     import torch
@@ -78,7 +78,7 @@ def test_merge_partition_bit_exact(cuda, ipt, mat):
     P = Plan(drp, dcol, dval, len(x), kernel="merge", items_per_thread=ipt)
     rows, nzs = P.partition()
     P.close()
-    ref_rows, ref_nzs = O.merge_path_split(rp.astype(np.int32), 256 * ipt, len(rows) - 1)
+    ref_rows, ref_nzs = O.merge_path_split(rp.astype(np.int32), 32 * ipt, len(rows) - 1)
     assert np.array_equal(rows, ref_rows) and np.array_equal(nzs, ref_nzs)
 
 
@@ -103,6 +103,17 @@ def test_bad_column_is_flagged_not_faulted(cuda):
     with pytest.raises(SbbError):
         P.check()
     P.close()
+
+
+def test_bad_column_rejected_by_tiled_plan(cuda):
+    """The tiled kernel range-checks columns once, when its plan copies them."""
+    from sbb.device import Plan, SbbError
+    rp, col, val, x, y = MATS["uniform"]()
+    col = col.copy()
+    col[-1] = -3
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    with pytest.raises(SbbError):
+        Plan(drp, dcol, dval, len(x), kernel="tiled")
 
 
 def test_bad_rowptr_rejected_at_plan(cuda):
