@@ -288,6 +288,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     p.m = hm;
     p.n = n;
     p.nnz = (int)(rp[hr1 + 1] - rp[hr0]);
+    p.base = (int)rp[hr0];
     p.rowptr = d_rp + hr0;
     p.col = d_col;
     p.val = d_val;

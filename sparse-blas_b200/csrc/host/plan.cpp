@@ -170,7 +170,8 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
         if ((rc = dalloc(&p->queue, 2, s, &p->scratch_bytes))) return rc;
         SBB_CUDA(cudaMemsetAsync(p->queue, 0, 2 * sizeof(unsigned), s));
         if (tiles > 0) {
-            launch_merge_partition(p->rowptr, p->m, items, p->tiles, p->tile_row, p->tile_nnz, s);
+            launch_merge_partition(p->rowptr, p->m, p->base, p->nnz, items, p->tiles, p->tile_row,
+                                   p->tile_nnz, s);
             if ((rc = carry_runs_build(p->tile_row + 1, p->tiles, p->m, &p->runs, s))) return rc;
             p->scratch_bytes += p->runs.bytes;
         }
@@ -225,7 +226,7 @@ int plan_run(Plan *p, double alpha, const void *x, double beta, double *y, cudaS
                           p->status, s);
         break;
     case SBB_KERNEL_MERGE: {
-        MergeScratch S{p->tile_row, p->tile_nnz, p->carry_val, &p->runs, p->tiles,
+        MergeScratch S{p->tile_row, p->tile_nnz, p->carry_val, &p->runs, nullptr, p->tiles,
                        p->queue, p->persistent_ctas};
         if (p->f32)
             launch_merge_f32(A, p->ipt, S, alpha, static_cast<const float *>(x), beta, y,

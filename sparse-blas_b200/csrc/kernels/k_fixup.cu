@@ -59,7 +59,7 @@ __global__ void runs_mark_kernel(const int *__restrict__ crow, int T, int m,
 __global__ void __launch_bounds__(FT)
 fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cval, int T,
              const int *__restrict__ run_first, const int *__restrict__ run_len, int short_blocks,
-             double alpha, double *__restrict__ y, unsigned *queue)
+             double alpha, double *__restrict__ y, unsigned *queue, const int *dev_count)
 {
     if (blockIdx.x < short_blocks) {
         int t = blockIdx.x * FT + threadIdx.x;
@@ -72,17 +72,22 @@ fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cva
         return;
     }
     __shared__ double s[FT];
-    const int j = blockIdx.x - short_blocks;
-    const int first = run_first[j], len = run_len[j];
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < len; i += FT) acc += cval[first + i];
-    s[threadIdx.x] = acc;
-    __syncthreads();
-    for (int w = FT / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    // with a device-side count, a fixed set of blocks strides over the runs
+    const int n_runs = dev_count ? *dev_count : (int)(gridDim.x - short_blocks);
+    const int stride = dev_count ? (int)(gridDim.x - short_blocks) : n_runs;
+    for (int j = blockIdx.x - short_blocks; j < n_runs; j += stride) {
+        const int first = run_first[j], len = run_len[j];
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < len; i += FT) acc += cval[first + i];
+        s[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = FT / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) y[crow[first]] += alpha * s[0];
         __syncthreads();
     }
-    if (threadIdx.x == 0) y[crow[first]] += alpha * s[0];
 }
 
 }  // namespace
@@ -124,13 +129,22 @@ void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async)
     R->n_runs = 0;
 }
 
+void launch_runs_mark(const int *crow, int T, int m, int *run_first, int *run_len,
+                      int *dev_count, cudaStream_t s)
+{
+    if (T > 0)
+        runs_mark_kernel<<<(T + FT - 1) / FT, FT, 0, s>>>(crow, T, m, run_first, run_len, dev_count);
+}
+
 void launch_fixup(int m, const int *crow, const double *cval, int T, const CarryRuns &R,
-                  double alpha, double *y, unsigned *queue, cudaStream_t s)
+                  double alpha, double *y, unsigned *queue, cudaStream_t s, const int *dev_count)
 {
     if (T <= 0) return;
     int short_blocks = (T + FT - 1) / FT;
-    fixup_kernel<<<short_blocks + R.n_runs, FT, 0, s>>>(m, crow, cval, T, R.run_first, R.run_len,
-                                                        short_blocks, alpha, y, queue);
+    int long_blocks = dev_count ? 148 : R.n_runs;
+    fixup_kernel<<<short_blocks + long_blocks, FT, 0, s>>>(m, crow, cval, T, R.run_first,
+                                                           R.run_len, short_blocks, alpha, y,
+                                                           queue, dev_count);
 }
 
 }  // namespace sbb

@@ -51,15 +51,15 @@ __device__ __forceinline__ void path_search(const int *rowptr, int m, long long 
     nz = (int)(base + d - lo);
 }
 
-__global__ void merge_partition_kernel(const int *__restrict__ rowptr, int m,
-                                       long long items, int tiles,
+// base / nnz come from the host (rowptr[0] and rowptr[m] of a valid matrix),
+// so even a corrupt row pointer cannot move a segment outside [base, base+nnz).
+__global__ void merge_partition_kernel(const int *__restrict__ rowptr, int m, int base,
+                                       long long nnz, long long items, int tiles,
                                        int *__restrict__ tile_row,
                                        int *__restrict__ tile_nnz)
 {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p > tiles) return;
-    int base = __ldg(rowptr);
-    long long nnz = (long long)__ldg(rowptr + m) - base;
     long long total = (long long)m + nnz;
     long long d = (long long)p * items;
     if (d > total) d = total;
@@ -155,6 +155,10 @@ __device__ __forceinline__ void merge_segment(
         if (i < nrows) {
             lo = i == 0 ? 0 : s_re[i - 1] - k0;  // row r0 may have started before k0
             hi = s_re[i] - k0;
+            // a valid row pointer keeps 0 <= lo <= hi <= nz; clamping makes a
+            // corrupt one harmless (wrong sums, no out-of-range reads)
+            lo = min(max(lo, 0), nz);
+            hi = min(max(hi, lo), nz);
         }
         const bool is_long = hi - lo > kLongRow;
         if (i < nrows && !is_long) {
@@ -182,7 +186,7 @@ __device__ __forceinline__ void merge_segment(
         }
     }
     // 3. carry: the part of row r1 inside this segment
-    const int clo = nrows > 0 ? s_re[nrows - 1] - k0 : 0;
+    const int clo = nrows > 0 ? min(max(s_re[nrows - 1] - k0, 0), nz) : 0;
     const double c = warp_range_sum<ACC>(s_p, clo, nz, lane);
     if (lane == 0) carry_val[w] = c;
     __syncwarp();  // shared memory is reused by this warp's next segment
@@ -230,7 +234,8 @@ void launch_merge_t(const CsrView &A, const MergeScratch &S, double alpha,
                                                        S.tile_row, S.tile_nnz, S.carry_val,
                                                        S.tiles, status);
         hook_stop(s);
-        launch_fixup(A.m, S.tile_row + 1, S.carry_val, S.tiles, *S.runs, alpha, y, nullptr, s);
+        launch_fixup(A.m, S.tile_row + 1, S.carry_val, S.tiles, *S.runs, alpha, y, nullptr, s,
+                     S.runs_count);
     }
 }
 
@@ -277,12 +282,12 @@ int merge_max_ctas_per_sm(int ipt, bool f32)
 #undef SBB_OCC
 }
 
-void launch_merge_partition(const int *rowptr, int m, long long items, int tiles,
-                            int *tile_row, int *tile_nnz, cudaStream_t s)
+void launch_merge_partition(const int *rowptr, int m, int base, long long nnz, long long items,
+                            int tiles, int *tile_row, int *tile_nnz, cudaStream_t s)
 {
     int n = tiles + 1;
-    merge_partition_kernel<<<(n + 255) / 256, 256, 0, s>>>(rowptr, m, items, tiles, tile_row,
-                                                           tile_nnz);
+    merge_partition_kernel<<<(n + 255) / 256, 256, 0, s>>>(rowptr, m, base, nnz, items, tiles,
+                                                           tile_row, tile_nnz);
 }
 
 void launch_merge(const CsrView &A, int ipt, const MergeScratch &S, double alpha,

@@ -63,19 +63,25 @@ struct CarryRuns {
 };
 int carry_runs_build(const int *carry_row, int T, int m, CarryRuns *R, cudaStream_t s);
 void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async);
+// Marks the runs on the device only; the count stays in *dev_count.
+void launch_runs_mark(const int *carry_row, int T, int m, int *run_first, int *run_len,
+                      int *dev_count, cudaStream_t s);
 // Adds the carries to y in a fixed order; also rearms `queue` when non-null.
+// dev_count non-null: the run count is read on the device (R.n_runs unused).
 void launch_fixup(int m, const int *carry_row, const double *carry_val, int T,
-                  const CarryRuns &R, double alpha, double *y, unsigned *queue, cudaStream_t s);
+                  const CarryRuns &R, double alpha, double *y, unsigned *queue, cudaStream_t s,
+                  const int *dev_count = nullptr);
 
 // K2: merge path.  One warp per segment of 32*IPT merge items.
 int merge_ipt_supported(int ipt);
 long long merge_items_per_tile(int ipt);
-void launch_merge_partition(const int *rowptr, int m, long long items, int tiles,
-                            int *tile_row, int *tile_nnz, cudaStream_t s);
+void launch_merge_partition(const int *rowptr, int m, int base, long long nnz, long long items,
+                            int tiles, int *tile_row, int *tile_nnz, cudaStream_t s);
 struct MergeScratch {
     const int *tile_row, *tile_nnz;   // tiles+1 coordinates; tile t carries row tile_row[t+1]
     double *carry_val;                // tiles
     const CarryRuns *runs;
+    const int *runs_count;            // non-null: run count kept on the device
     int tiles;
     unsigned *queue;                  // persistent form: [0] = next tile, [1] = done
     int persistent_ctas;              // 0 = one CTA per tile
@@ -97,6 +103,7 @@ void launch_pieces(const long long *lo, const long long *hi, int npieces,
 // Plan object behind sbb_plan_t.
 struct Plan {
     int m = 0, n = 0, nnz = 0;
+    int base = 0;            // rowptr[0] (non-zero for a row range of a larger matrix)
     const int *rowptr = nullptr, *col = nullptr;
     const void *val = nullptr;
     bool f32 = false;
