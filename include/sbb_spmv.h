@@ -137,6 +137,24 @@ int sbb_plan_info_get(sbb_plan_t plan, sbb_plan_info *info);
 int sbb_plan_partition(sbb_plan_t plan, int *h_row, int *h_nnz, int cap);
 int sbb_plan_destroy(sbb_plan_t plan);
 
+/* Merge-path y = alpha*A*x + beta*y on device arrays that allocates nothing:
+ * no counterpart in the reference.  For callers that must not call cudaMalloc
+ * (a memory-capped or pre-partitioned process, a callback or real-time path
+ * that may not block on the allocator, a host framework that owns all device
+ * memory), the scratch lives in a fixed 5 MiB __device__ array of the library,
+ * held on every GPU that loads it until the process exits.  Limit:
+ * m + nnz <= 100,663,296 (larger inputs return SBB_ERR_ARG).  All calls share
+ * that array and it keeps the last call's contents, so calls that overlap on
+ * the GPU race; serialise them.  The first call on a device looks up the
+ * array's address; make it before any stream capture on that device.  The row
+ * pointer must start at 0 and end at nnz; invalid indices are not reported by
+ * this entry point (they cannot make it read out of range).  Asynchronous on
+ * `stream` (a cudaStream_t or NULL). */
+int sbb_spmv_merge_noalloc(int m, int n, int nnz, const int *d_rowptr,
+                           const int *d_col, const double *d_val, double alpha,
+                           const double *d_x, double beta, double *d_y,
+                           void *stream);
+
 const char *sbb_last_error(void);
 
 #ifdef __cplusplus

@@ -70,6 +70,8 @@ SIGNATURES = {
     "sbb_plan_info_get": (C.c_int, [vp, C.POINTER(PlanInfo)]),
     "sbb_plan_partition": (C.c_int, [vp, vp, vp, C.c_int]),
     "sbb_plan_destroy": (C.c_int, [vp]),
+    "sbb_spmv_merge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_double, vp,
+                                         C.c_double, vp, vp]),
     "sbb_last_error": (C.c_char_p, []),
 }
 
