@@ -8,6 +8,7 @@
 // matrices whose row lengths are close to V; long rows serialise on one group.
 #include "../sbb_internal.h"
 #include "common.cuh"
+#include "spmv_device.cuh"
 
 namespace sbb {
 
@@ -21,40 +22,15 @@ vector_kernel(int m, int n, const int *__restrict__ rowptr, const int *__restric
               const typename PT::V *__restrict__ val, const typename PT::V *__restrict__ x,
               double *__restrict__ y, double alpha, double beta, unsigned *status)
 {
-    const int lane = threadIdx.x & (V - 1);
     const int group = (blockIdx.x * VT + threadIdx.x) / V;
     const int groups = gridDim.x * (VT / V);
     unsigned bad = 0;
     // The trip count is uniform across the warp (all its groups step together)
-    // so the full-mask shuffles below always see all 32 lanes.
+    // so the full-mask shuffles always see all 32 lanes.
     const int warp_first = group - ((threadIdx.x & 31) / V);
     for (int base = warp_first; base < m; base += groups) {
         const int row = base + (group - warp_first);
-        const bool active = row < m;
-        int lo = 0, hi = 0;
-        if (active) {
-            lo = __ldg(rowptr + row);
-            hi = __ldg(rowptr + row + 1);
-        }
-        ACC acc;
-        acc.zero();
-        int k = lo + lane;
-        // two independent loads in flight per lane
-        for (; k + V < hi; k += 2 * V) {
-            int c0 = ld_stream(col + k), c1 = ld_stream(col + k + V);
-            auto v0 = ld_stream(val + k), v1 = ld_stream(val + k + V);
-            auto x0 = gather_x(x, c0, n, bad), x1 = gather_x(x, c1, n, bad);
-            acc.add(PT::make(v0, x0));
-            acc.add(PT::make(v1, x1));
-        }
-        if (k < hi) acc.add(PT::make(ld_stream(val + k), gather_x(x, ld_stream(col + k), n, bad)));
-        double sum = acc.get();
-#pragma unroll
-        for (int o = V / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, V);
-        if (active && lane == 0) {
-            double *yp = y + row;
-            __stcs(yp, axpby(alpha, sum, beta, yp));
-        }
+        vector_row<PT, ACC, V>(row, row < m, n, rowptr, col, val, x, y, alpha, beta, bad);
     }
     if (bad) atomicOr(status, ST_BAD_COL);
 }
