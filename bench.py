@@ -1,7 +1,7 @@
 """Benchmark: FP64 CSR SpMV HBM throughput on the large irregular matrix.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sbb|reference]
-                    [--kernel merge|vector|tiled|auto] [--workload c2|c3|c1]
+                    [--kernel merge|vector|tiled|auto] [--workload c2|c3|c1|c5]
 
 Workload (default): the 5.5M-row irregular matrix (c2_circuit_5.5M: m = n =
 5.5M, nnz ~ 60M, diagonal + band + power-law long-range entries, 550 dense
@@ -16,6 +16,11 @@ metric through the reference-facing C ABI (spMV_mgpu_v1, kernel 2) with host
 buffers in pinned memory: every step copies the matrix, x and y to the GPU and
 y back.  Multi-GPU runs are independent replicas (one per rank, no
 collective); ``value`` sums the ranks' bytes over the slowest rank's time.
+
+``--workload c5`` prints the batched form's line instead: 512 seeded
+matrices (banded / power-law / block-diagonal), each matrix's plain launches
+one after another vs one graph-captured persistent launch over all of them,
+with the heuristic's and the exhaustive autotuner's kernel classes.
 
 ``--impl reference`` times the reference's host CSR SpMV (main.cu:350-356,
 restated with +beta*y in oracle/sbb_oracle.c) on all host cores over a bounded
@@ -207,6 +212,147 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def default_class(A):
+    """The plain path's heuristic (default_kernel_choice in csrc/host/plan.cpp)
+    on the batch classes: vector CSR with V = next power of two >= mean row
+    length (4..32) when rows are short and even, the sigma = 4 tiles
+    otherwise."""
+    L = np.diff(A.rowptr)
+    mean = float(L.mean()) if len(L) else 0.0
+    v, cls = 4, 0
+    while v < 32 and v < mean:
+        v <<= 1
+        cls += 1
+    mx = int(L.max()) if len(L) else 0
+    return cls if (mx <= 4 * v and mx <= 128) else 5
+
+
+C5_DESC = ("c5: {count} matrices, n log-uniform [1k,200k], banded / power-law / block-diagonal "
+           "thirds, nnz/row log-uniform [4,200], alpha=1, beta=0.5")
+
+
+def c5_matrices(count, dev):
+    """The batch: matrix i from seed 5+i, x and y from seeds 5000+i / 6000+i."""
+    import torch
+    from sbb import gen
+    mats, total = [], 0
+    for i in range(count):
+        A = gen.c5(i)
+        x = gen.uniform_vec(5000 + i, A.n)
+        y = gen.uniform_vec(6000 + i, A.m)
+        d = dict(m=A.m, n=A.n, alpha=1.0, beta=0.5, A=A, x_h=x, y_h=y)
+        if dev is not None:
+            d.update(rowptr=torch.from_numpy(A.rowptr32()).to(dev),
+                     col=torch.from_numpy(A.col).to(dev), val=torch.from_numpy(A.val).to(dev),
+                     x=torch.from_numpy(x).to(dev), y=torch.from_numpy(y).to(dev))
+        total += algo_bytes(A.m, A.n, A.nnz)
+        mats.append(d)
+    return mats, total
+
+
+def run_batch(args, ws, rank, local):
+    """c5: 512 matrices; per-matrix plain launches vs one graph-captured
+    persistent launch, with the heuristic's and the exhaustive autotuner's
+    classes."""
+    import torch
+    from sbb.batch import Batch, tune
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    count = args.batch_count
+    t_gen = time.perf_counter()
+    mats, total_bytes = c5_matrices(count, dev)
+    t_gen = time.perf_counter() - t_gen
+    # exhaustive autotune: every class on every matrix, as plain launches
+    t_tune = time.perf_counter()
+    times = np.array([tune(d, reps=3) for d in mats])
+    t_tune = time.perf_counter() - t_tune
+    best = [int(np.argmin(t)) for t in times]
+    default = [default_class(d["A"]) for d in mats]
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    res = {}
+    for name, classes in (("default", default), ("tuned", best)):
+        B = Batch(mats, classes)
+        res[f"each_{name}_ms"] = timed(B.run_each, args.batch_reps)
+        res[f"batch_{name}_ms"] = timed(B.run_graph, args.batch_reps)
+        B.check()
+        res[f"launches_each_{name}"] = B.launches(per_matrix=True)
+        B.close()
+    best_sum = float(times.min(axis=1).sum())
+    pick = lambda cls: float(sum(times[i, c] for i, c in enumerate(cls)))  # noqa: E731
+    ms = max_over_ranks(res["batch_tuned_ms"], ws)
+    value = total_bytes * ws / (ms * 1e-3) / 1e9
+    if rank != 0:
+        return
+    line = {
+        "metric": "batched SpMV GB/s (FP64 CSR matrices, one graph-captured persistent launch)",
+        "value": round(value, 3), "unit": "GB/s", "n_gpus": ws, "steps": args.batch_reps,
+        "warmup": 3, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": C5_DESC.format(count=count),
+                   "bytes_per_step": total_bytes, "l2_flush": "no (12.5 GB working set > L2)",
+                   "gen_s": round(t_gen, 1), "tune_s": round(t_tune, 1),
+                   "classes_tuned": np.bincount(best, minlength=6).tolist(),
+                   "classes_default": np.bincount(default, minlength=6).tolist(),
+                   "speedup_batch_vs_each_default": round(res["each_default_ms"] / ms, 3),
+                   "speedup_batch_vs_each_tuned": round(res["each_tuned_ms"] / ms, 3),
+                   "regret_default": round(pick(default) / best_sum - 1, 4),
+                   **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in res.items()}},
+        "gpu_launches": 2 * args.batch_reps,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_batch(args, ws, rank):
+    """The reference's host loop over the c5 matrices, all host cores, until
+    the CPU budget is spent (bounded sample: the first k matrices)."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = os.cpu_count() or 1
+    mats, _ = c5_matrices(args.batch_count, None)
+    done_bytes, t_total, k = 0, 0.0, 0
+    for d in mats:
+        A = d["A"]
+        y = d["y_h"].copy()
+        rp = np.ascontiguousarray(A.rowptr)
+        t0 = time.perf_counter()
+        O.spmv_host(rp, A.col, A.val, d["x_h"], 1.0, 0.5, y, threads)
+        t_total += time.perf_counter() - t0
+        done_bytes += algo_bytes(A.m, A.n, A.nnz)
+        k += 1
+        if t_total >= args.cpu_budget:
+            break
+    gbs = done_bytes / t_total / 1e9
+    line = {
+        "metric": "batched SpMV GB/s (FP64 CSR matrices, one graph-captured persistent launch)",
+        "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": 1, "warmup": 0, "ms_per_step": round(t_total * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": C5_DESC.format(count=args.batch_count),
+                                        "threads": threads},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"the first {k} matrices, one pass each"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_sbb(args, ws, rank, local):
     import ctypes as C
     import torch
@@ -340,7 +486,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="sbb", choices=["sbb", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--batch-count", type=int, default=512, help="c5: matrices in the batch")
+    ap.add_argument("--batch-reps", type=int, default=20, help="c5: timed batch runs")
     ap.add_argument("--kernel", default="tiled", choices=["merge", "vector", "tiled", "auto"])
     ap.add_argument("--ipt", type=int, default=6)
     ap.add_argument("--persistent", type=int, default=0)
@@ -354,7 +502,9 @@ def main():
     ws, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
-            run_reference(args, ws, rank)
+            (run_reference_batch if args.workload == "c5" else run_reference)(args, ws, rank)
+        elif args.workload == "c5":
+            run_batch(args, ws, rank, local)
         else:
             run_sbb(args, ws, rank, local)
     finally:

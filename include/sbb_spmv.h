@@ -137,6 +137,56 @@ int sbb_plan_info_get(sbb_plan_t plan, sbb_plan_info *info);
 int sbb_plan_partition(sbb_plan_t plan, int *h_row, int *h_nnz, int cap);
 int sbb_plan_destroy(sbb_plan_t plan);
 
+/* ---- batched form: many matrices, one persistent launch ----------------- */
+
+/* Kernel classes a matrix of a batch can use (the autotuner's and the
+ * learned selector's choices; each computes the same SpMV):
+ *   0..3: vector CSR with 4, 8, 16, 32 lanes per row;
+ *   4:    merge path, 6 items per lane (192-item warp segments);
+ *   5:    CSR5-style tiles of 32 x 4 nnz (sigma = 4).
+ * No counterpart in the reference, whose v2 driver runs the tasks of ONE
+ * matrix from a host pool (SparseBLAS/src/dspmv_mgpu_v2.cu:73-188). */
+#define SBB_NUM_CLASSES 6
+
+typedef struct {
+    int m, n, nnz;
+    const int *rowptr, *col;   /* device, int32, rowptr[0] == 0 */
+    const double *val;         /* device, FP64 */
+    const double *x;           /* device */
+    double *y;                 /* device; y = alpha*A*x + beta*y */
+    double alpha, beta;
+    int cls;                   /* 0 .. SBB_NUM_CLASSES-1 */
+} sbb_batch_item;
+
+typedef struct sbb_batch_s *sbb_batch_t;
+
+/* Builds one plan per matrix (validating each) and the device work list.
+ * The arrays must stay valid while the batch lives. */
+int sbb_batch_create(sbb_batch_t *batch, const sbb_batch_item *items, int count,
+                     void *stream);
+/* All SpMVs of the batch in one persistent launch: warps take work units
+ * (row chunks, merge segments or tile groups) from a device queue; one more
+ * launch adds the carries of every merge/tiled matrix and finishes the empty
+ * rows of tiled ones.  Each matrix's y is bit-identical to
+ * sbb_batch_run_each with the same classes.  The y arrays must not overlap. */
+int sbb_batch_run(sbb_batch_t batch, void *stream);
+/* Same launches, captured once in a CUDA graph and replayed. */
+int sbb_batch_run_graph(sbb_batch_t batch, void *stream);
+/* The baseline: each matrix's own plain launch sequence, one after another. */
+int sbb_batch_run_each(sbb_batch_t batch, void *stream);
+/* Kernel launches of one run: per_matrix = 0 -> batched, 1 -> run_each. */
+int sbb_batch_launches(sbb_batch_t batch, int per_matrix);
+/* Synchronise the status words: SBB_OK or SBB_ERR_INPUT. */
+int sbb_batch_check(sbb_batch_t batch);
+int sbb_batch_destroy(sbb_batch_t batch);
+
+/* Autotuner probe: mean time (ms, CUDA events, `reps` runs after one warm-up)
+ * of each class on one matrix as a plain launch; d_y is overwritten.  ms has
+ * SBB_NUM_CLASSES entries. */
+int sbb_tune_classes(int m, int n, int nnz, const int *d_rowptr, const int *d_col,
+                     const double *d_val, const double *d_x, double *d_y, double alpha,
+                     double beta, int reps, float *ms, void *stream);
+
 /* Merge-path y = alpha*A*x + beta*y on device arrays that allocates nothing:
  * no counterpart in the reference.  For callers that must not call cudaMalloc
  * (a memory-capped or pre-partitioned process, a callback or real-time path

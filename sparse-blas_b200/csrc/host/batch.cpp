@@ -1,0 +1,369 @@
+// batch.cpp — batched SpMV (one persistent launch, optionally a CUDA graph)
+// and the per-matrix class timer the autotuner uses.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../sbb_internal.h"
+
+using namespace sbb;
+
+struct sbb_batch_s {
+    std::vector<Plan *> plans;
+    std::vector<BatchMat> host_mats;
+    BatchMat *d_mats = nullptr;
+    long long *d_unit0 = nullptr;
+    unsigned long long *d_queue = nullptr;  // [0]: next claim of kBatchClaim units
+    unsigned *d_status = nullptr;
+    long long total = 0;
+    // carry fix-up of the merge/tiled-class matrices, empty rows of tiled ones
+    BatchFix fix{};
+    long long fix_slots = 0;
+    long long *d_tile0 = nullptr;
+    int *d_fix_mat = nullptr, *d_run_mat = nullptr, *d_run_first = nullptr, *d_run_len = nullptr;
+    int *d_empty_row = nullptr, *d_empty_mat = nullptr;
+    int grid = 0, device = 0;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+// The plain-plan configuration of each class.
+static sbb_config class_config(int cls)
+{
+    sbb_config c{};
+    if (cls == kBatchMergeClass) {
+        c.kernel = SBB_KERNEL_MERGE;
+        c.items_per_thread = kBatchIpt;
+    } else if (cls == kBatchTiledClass) {
+        c.kernel = SBB_KERNEL_TILED;
+        c.tile_sigma = kBatchSigma;
+    } else {
+        c.kernel = SBB_KERNEL_VECTOR;
+        c.vector_width = 4 << cls;
+    }
+    return c;
+}
+
+static void batch_free(sbb_batch_s *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    void *ptrs[] = {b->d_mats,    b->d_unit0,     b->d_queue,      b->d_status,
+                    b->d_tile0,   b->d_fix_mat,   b->d_run_mat,    b->d_run_first,
+                    b->d_run_len, b->d_empty_row, b->d_empty_mat};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (Plan *p : b->plans) {
+        plan_free(p);
+        delete p;
+    }
+    delete b;
+}
+
+static int enqueue(sbb_batch_s *b, cudaStream_t s)
+{
+    const int n = (int)b->host_mats.size();
+    SBB_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), s));
+    launch_batch(b->d_mats, n, b->d_unit0, b->total, b->d_queue, b->d_status, b->grid, s);
+    launch_batch_fixup(b->d_mats, b->fix, b->fix_slots, s);
+    SBB_CUDA(cudaGetLastError());
+    return SBB_OK;
+}
+
+extern "C" {
+
+int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, void *stream)
+{
+    if (!out || count < 0 || (count > 0 && !items)) {
+        set_error("bad sbb_batch_create arguments");
+        return SBB_ERR_ARG;
+    }
+    *out = nullptr;
+    auto s = static_cast<cudaStream_t>(stream);
+    auto *b = new sbb_batch_s();
+    cudaGetDevice(&b->device);
+    std::vector<long long> unit0(count + 1, 0);
+    std::vector<long long> tile0(1, 0);
+    std::vector<int> fix_mat, run_mat, run_first, run_len, empty_row, empty_mat;
+    // copies cnt ints from the device; false (error set) on failure
+    auto fetch = [&](std::vector<int> &h, const int *d, int cnt) {
+        h.resize(cnt);
+        if (cnt == 0) return true;
+        if (cudaMemcpyAsync(h.data(), d, sizeof(int) * cnt, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            set_error("batch: copy of plan metadata failed");
+            return false;
+        }
+        return true;
+    };
+    // carries of one merge/tiled matrix: its slots and multi-slot runs
+    auto add_carries = [&](int i, int slots, const CarryRuns &R) {
+        if (slots <= 0) return true;
+        fix_mat.push_back(i);
+        tile0.push_back(tile0.back() + slots);
+        std::vector<int> f, l;
+        if (!fetch(f, R.run_first, R.n_runs) || !fetch(l, R.run_len, R.n_runs)) return false;
+        for (int r = 0; r < R.n_runs; r++) {
+            run_mat.push_back(i);
+            run_first.push_back(f[r]);
+            run_len.push_back(l[r]);
+        }
+        return true;
+    };
+    for (int i = 0; i < count; i++) {
+        const sbb_batch_item &it = items[i];
+        if (it.cls < 0 || it.cls >= SBB_NUM_CLASSES || it.m < 0 || it.n < 0 || it.nnz < 0 ||
+            !it.rowptr || (it.nnz > 0 && (!it.col || !it.val || !it.x)) || (it.m > 0 && !it.y)) {
+            set_error("bad batch item " + std::to_string(i));
+            batch_free(b);
+            return SBB_ERR_ARG;
+        }
+        auto *p = new Plan();
+        p->m = it.m;
+        p->n = it.n;
+        p->nnz = it.nnz;
+        p->rowptr = it.rowptr;
+        p->col = it.col;
+        p->val = it.val;
+        b->plans.push_back(p);
+        sbb_config c = class_config(it.cls);
+        int rc = plan_build(p, &c, s);
+        if (rc != SBB_OK) {
+            cudaStreamSynchronize(s);
+            batch_free(b);
+            return rc;
+        }
+        BatchMat M{};
+        M.rowptr = it.rowptr;
+        M.col = it.col;
+        M.val = it.val;
+        M.x = it.x;
+        M.y = it.y;
+        M.m = it.m;
+        M.n = it.n;
+        M.cls = it.cls;
+        M.alpha = it.alpha;
+        M.beta = it.beta;
+        M.nnz = it.nnz;
+        long long units;
+        if (it.cls == kBatchMergeClass) {
+            M.tile_row = p->tile_row;
+            M.tile_nnz = p->tile_nnz;
+            M.crow = p->tile_row + 1;  // segment t carries into the row it ends in
+            M.carry_val = p->carry_val;
+            M.tiles = p->tiles;
+            units = p->tiles;
+            if (!add_carries(i, p->tiles, p->runs)) {
+                batch_free(b);
+                return SBB_ERR_CUDA;
+            }
+        } else if (it.cls == kBatchTiledClass) {
+            TiledView v{};
+            if (!tiled_view(p, &v) || v.sigma != kBatchSigma) {
+                set_error("batch: tiled plan missing");
+                batch_free(b);
+                return SBB_ERR_CUDA;
+            }
+            M.blob = v.blob;
+            M.tile_seg = v.tile_seg;
+            M.ne = v.ne;
+            M.crow = v.carry_row;
+            M.carry_val = v.carry_val;
+            M.tiles = v.tiles;
+            units = (v.tiles + kBatchTileGroup - 1) / kBatchTileGroup;
+            std::vector<int> e;
+            if (!add_carries(i, v.tiles, *v.runs) || !fetch(e, v.empty, v.n_empty)) {
+                batch_free(b);
+                return SBB_ERR_CUDA;
+            }
+            for (int r : e) {
+                empty_row.push_back(r);
+                empty_mat.push_back(i);
+            }
+        } else {
+            // units of about kBatchVectorNnz nnz: vsteps chunks of cr rows
+            const long long cr = vector_chunk_rows(4 << it.cls, kBatchVectorU);
+            const double mean = it.m > 0 ? (double)it.nnz / it.m : 1.0;
+            long long steps = (long long)(kBatchVectorNnz / (cr * std::max(mean, 1.0)) + 0.5);
+            steps = std::min<long long>(64, std::max<long long>(1, steps));
+            M.vsteps = (int)steps;
+            const long long rows_per_unit = cr * steps;
+            units = (it.m + rows_per_unit - 1) / rows_per_unit;
+        }
+        b->host_mats.push_back(M);
+        unit0[i + 1] = unit0[i] + units;
+    }
+    b->total = unit0[count];
+    auto fail = [&](cudaError_t e) {
+        set_error(std::string("batch setup: ") + cudaGetErrorString(e));
+        batch_free(b);
+        return SBB_ERR_CUDA;
+    };
+    cudaError_t e;
+    const int nfix = (int)fix_mat.size(), nruns = (int)run_mat.size();
+    const int nempty = (int)empty_row.size();
+    if ((e = cudaMalloc(&b->d_mats, sizeof(BatchMat) * std::max(count, 1))) ||
+        (e = cudaMalloc(&b->d_unit0, sizeof(long long) * (count + 1))) ||
+        (e = cudaMalloc(&b->d_queue, sizeof(unsigned long long))) ||
+        (e = cudaMalloc(&b->d_status, sizeof(unsigned))) ||
+        (e = cudaMalloc(&b->d_tile0, sizeof(long long) * (nfix + 1))) ||
+        (e = cudaMalloc(&b->d_fix_mat, sizeof(int) * std::max(nfix, 1))) ||
+        (e = cudaMalloc(&b->d_run_mat, sizeof(int) * std::max(nruns, 1))) ||
+        (e = cudaMalloc(&b->d_run_first, sizeof(int) * std::max(nruns, 1))) ||
+        (e = cudaMalloc(&b->d_run_len, sizeof(int) * std::max(nruns, 1))) ||
+        (e = cudaMalloc(&b->d_empty_row, sizeof(int) * std::max(nempty, 1))) ||
+        (e = cudaMalloc(&b->d_empty_mat, sizeof(int) * std::max(nempty, 1))))
+        return fail(e);
+    auto up = [&](void *dst, const void *src, size_t bytes) {
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s) : cudaSuccess;
+    };
+    if ((e = up(b->d_tile0, tile0.data(), sizeof(long long) * (nfix + 1))) ||
+        (e = up(b->d_fix_mat, fix_mat.data(), sizeof(int) * nfix)) ||
+        (e = up(b->d_run_mat, run_mat.data(), sizeof(int) * nruns)) ||
+        (e = up(b->d_run_first, run_first.data(), sizeof(int) * nruns)) ||
+        (e = up(b->d_run_len, run_len.data(), sizeof(int) * nruns)) ||
+        (e = up(b->d_empty_row, empty_row.data(), sizeof(int) * nempty)) ||
+        (e = up(b->d_empty_mat, empty_mat.data(), sizeof(int) * nempty)) ||
+        (e = up(b->d_mats, b->host_mats.data(), sizeof(BatchMat) * count)) ||
+        (e = up(b->d_unit0, unit0.data(), sizeof(long long) * (count + 1))) ||
+        (e = cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s)) ||
+        (e = cudaStreamSynchronize(s)))
+        return fail(e);
+    b->fix = BatchFix{b->d_tile0,   b->d_fix_mat, nfix,           b->d_run_mat,   b->d_run_first,
+                      b->d_run_len, nruns,        b->d_empty_row, b->d_empty_mat, nempty};
+    b->fix_slots = tile0.back();
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    b->grid = sms * std::max(batch_max_ctas_per_sm(), 1);
+    *out = b;
+    return SBB_OK;
+}
+
+int sbb_batch_run(sbb_batch_t b, void *stream)
+{
+    if (!b) return SBB_ERR_ARG;
+    return enqueue(b, static_cast<cudaStream_t>(stream));
+}
+
+int sbb_batch_run_graph(sbb_batch_t b, void *stream)
+{
+    if (!b) return SBB_ERR_ARG;
+    if (!b->exec) {
+        // capture on a private stream (the caller's may be the legacy default
+        // stream, which cannot be captured), replay on the caller's
+        if (!b->cap) SBB_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+        SBB_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue(b, b->cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+        if (rc != SBB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) {
+            set_error(std::string("graph capture: ") + cudaGetErrorString(e));
+            return SBB_ERR_CUDA;
+        }
+        b->graph = g;
+        SBB_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    SBB_CUDA(cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)));
+    return SBB_OK;
+}
+
+int sbb_batch_run_each(sbb_batch_t b, void *stream)
+{
+    if (!b) return SBB_ERR_ARG;
+    auto s = static_cast<cudaStream_t>(stream);
+    for (size_t i = 0; i < b->plans.size(); i++) {
+        const BatchMat &M = b->host_mats[i];
+        int rc = plan_run(b->plans[i], M.alpha, M.x, M.beta, M.y, s);
+        if (rc != SBB_OK) return rc;
+    }
+    return SBB_OK;
+}
+
+int sbb_batch_launches(sbb_batch_t b, int per_matrix)
+{
+    if (!b) return 0;
+    if (!per_matrix)
+        return (b->total > 0 ? 1 : 0) + (b->fix_slots > 0 || b->fix.n_empty > 0 ? 1 : 0);
+    int n = 0;
+    for (Plan *p : b->plans) n += plan_launches(p);
+    return n;
+}
+
+int sbb_batch_check(sbb_batch_t b)
+{
+    if (!b) return SBB_ERR_ARG;
+    unsigned st = 0;
+    SBB_CUDA(cudaMemcpy(&st, b->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+    for (Plan *p : b->plans) {
+        unsigned q = 0;
+        SBB_CUDA(cudaMemcpy(&q, p->status, sizeof(q), cudaMemcpyDeviceToHost));
+        st |= q;
+    }
+    if (st) {
+        set_error("batch: device status " + std::to_string(st) +
+                  ((st & ST_TIMEOUT) ? " (a bounded wait on a tile copy gave up)" : ""));
+        return SBB_ERR_INPUT;
+    }
+    return SBB_OK;
+}
+
+int sbb_batch_destroy(sbb_batch_t b)
+{
+    if (!b) return SBB_OK;
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    batch_free(b);
+    return SBB_OK;
+}
+
+int sbb_tune_classes(int m, int n, int nnz, const int *d_rowptr, const int *d_col,
+                     const double *d_val, const double *d_x, double *d_y, double alpha,
+                     double beta, int reps, float *ms, void *stream)
+{
+    if (!ms || reps <= 0 || m < 0 || n < 0 || nnz < 0 || !d_rowptr) {
+        set_error("bad sbb_tune_classes arguments");
+        return SBB_ERR_ARG;
+    }
+    auto s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    SBB_CUDA(cudaEventCreate(&e0));
+    SBB_CUDA(cudaEventCreate(&e1));
+    int rc = SBB_OK;
+    for (int cls = 0; cls < SBB_NUM_CLASSES && rc == SBB_OK; cls++) {
+        Plan p;
+        p.m = m;
+        p.n = n;
+        p.nnz = nnz;
+        p.rowptr = d_rowptr;
+        p.col = d_col;
+        p.val = d_val;
+        sbb_config c = class_config(cls);
+        rc = plan_build(&p, &c, s);
+        if (rc == SBB_OK) rc = plan_run(&p, alpha, d_x, beta, d_y, s);  // warm-up
+        if (rc == SBB_OK) {
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < reps && rc == SBB_OK; r++) rc = plan_run(&p, alpha, d_x, beta, d_y, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms[cls] = t / reps;
+        }
+        cudaStreamSynchronize(s);
+        plan_free(&p);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,302 @@
+// k_batch.cu — many SpMVs of uneven sizes in one persistent launch.
+//
+// The reference runs tasks from a host pool with an OpenMP thread per GPU
+// and q streams each (SparseBLAS/src/dspmv_mgpu_v2.cu:73-188).  Here the pool
+// is a device work queue: each matrix of the batch contributes work units -
+// row chunks for the vector-CSR classes, warp segments for the merge-path
+// class, groups of kBatchTileGroup tiles for the tiled class - and the warps
+// of one persistent grid claim kBatchClaim consecutive units per queue access
+// (one atomic on one counter) until the queue is empty.  A unit runs exactly
+// the device code the standalone kernel runs for it (spmv_device.cuh,
+// tiled_device.cuh), and the carries and empty rows of every merge/tiled
+// matrix are then finished by one fix-up launch with the standalone fix-up's
+// arithmetic, so every matrix's y is bit-identical to a standalone launch with
+// the same class.  A tiled unit is copied into shared memory with one TMA bulk
+// copy; while a warp reduces a unit, the copy of the next unit of its claim is
+// in flight, and the x values of each tile are gathered before the previous
+// tile is reduced.
+#include "../sbb_internal.h"
+#include "common.cuh"
+#include "spmv_device.cuh"
+#include "tiled_device.cuh"
+
+// CTAs per SM the batch kernel's register budget aims at.
+#ifndef SBB_BATCH_MINB
+#define SBB_BATCH_MINB 2
+#endif
+
+namespace sbb {
+
+namespace {
+
+constexpr int BT = 256;  // threads per CTA
+constexpr int BW = BT / 32;
+constexpr int SEG = 32 * kBatchIpt;
+constexpr uint32_t TBB = (uint32_t)tile_bytes_of(kBatchSigma, 8);
+constexpr int TG = kBatchTileGroup;
+constexpr uint32_t kBit0 = 32 * kBatchSigma * 12;  // offset of a tile's row-start bits
+constexpr size_t kMergeWarpBytes = sizeof(double) * SEG + sizeof(int) * (SEG + 1);
+constexpr size_t kTiledWarpBytes = 2 * (size_t)TG * TBB;  // two unit slots
+// per-warp shared memory (dynamic): a merge segment's staging or two tile slots
+constexpr size_t kWarpBytes =
+    ((kMergeWarpBytes > kTiledWarpBytes ? kMergeWarpBytes : kTiledWarpBytes) + 127) / 128 * 128;
+constexpr size_t kSmemBytes = BW * kWarpBytes;
+static_assert(TBB % 16 == 0, "bulk copies move multiples of 16 bytes");
+
+__device__ __forceinline__ unsigned char *warp_smem()
+{
+    extern __shared__ __align__(128) unsigned char s_dyn[];
+    return s_dyn + (size_t)(threadIdx.x >> 5) * kWarpBytes;
+}
+
+// A vector-class unit: vsteps consecutive chunks of CR rows (kBatchVectorU
+// rows of each lane group in flight: the batch kernel's register budget).
+template <int V>
+__device__ __forceinline__ void vector_unit(const BatchMat &M, int local, unsigned &bad)
+{
+    constexpr int U = kBatchVectorU;
+    constexpr int CR = VectorShape<V, U>::CR;
+    static_assert(CR == vector_chunk_rows(V, U), "host and device chunk sizes differ");
+    const uint64_t stream = l2_evict_first();
+    const long long r0 = (long long)local * CR * M.vsteps;
+    for (int s = 0; s < M.vsteps && r0 + (long long)CR * s < M.m; ++s)
+        vector_chunk<ProdF64, AccF64, V, U>((int)(r0 + (long long)CR * s), M.m, M.n, M.rowptr,
+                                            M.col, static_cast<const double *>(M.val), M.x, M.y,
+                                            M.alpha, M.beta, stream, bad);
+}
+
+__device__ __forceinline__ int find_matrix(const long long *unit0, int nmat, long long u)
+{
+    int lo = 0, hi = nmat - 1;  // last i with unit0[i] <= u
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(unit0 + mid) <= u)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Units of matrix i relative to the claim start u0: first (negative when the
+// matrix began before the claim) and last (clamped to the claim's n units).
+// A matrix has fewer than 2^31 units, so both fit an int.
+struct ClaimSpan {
+    int first, last;
+};
+__device__ __forceinline__ ClaimSpan claim_span(const long long *unit0, int i, long long u0, int n)
+{
+    const long long a = __ldg(unit0 + i) - u0, b = __ldg(unit0 + i + 1) - u0;
+    return ClaimSpan{(int)a, (int)(b < n ? b : n)};
+}
+
+__global__ void __launch_bounds__(BT, SBB_BATCH_MINB)
+batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__restrict__ unit0,
+             long long total, unsigned long long *queue, unsigned *status)
+{
+    __shared__ __align__(8) uint64_t bars[BW][2];
+    const int lane = threadIdx.x & 31;
+    const uint32_t bar0 = smem_u32(&bars[threadIdx.x >> 5][0]);
+    if (lane == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    // Whole warp: copy the tiles of unit `unit` of MM into slot `sl`.  The
+    // slot may have been written by the merge staging (generic proxy) before:
+    // every lane fences its writes against the async proxy before lane 0
+    // starts the copy.
+    auto issue = [&](const BatchMat &MM, int unit, int sl) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+            const int t0 = unit * TG;
+            const int nt = MM.tiles - t0 < TG ? MM.tiles - t0 : TG;
+            const uint32_t bytes = (uint32_t)nt * TBB;
+            mbar_expect_tx(bar0 + 8 * sl, bytes);
+            bulk_g2s(smem_u32(warp_smem() + sl * TG * TBB), MM.blob + (size_t)t0 * TBB, bytes,
+                     bar0 + 8 * sl, evict_first_policy());
+        }
+    };
+    uint32_t phases = 0u;  // bit s: parity of slot s's next phase
+    unsigned bad = 0, timeout = 0;
+    int pre_k = -1;  // claim position whose tile copy is in flight (into slot pre_s)
+    int pre_s = 0;
+    while (!timeout) {
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(queue, 1ull);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        const long long u0 = (long long)c * kBatchClaim;
+        if (u0 >= total) break;
+        const int n = (int)(total - u0 < kBatchClaim ? total - u0 : kBatchClaim);
+        int i = find_matrix(unit0, nmat, u0);
+        ClaimSpan sp = claim_span(unit0, i, u0, n);
+        for (int k = 0; k < n; ++k) {
+            while (k >= sp.last) {  // units are in matrix order
+                ++i;
+                sp = claim_span(unit0, i, u0, n);
+            }
+            const BatchMat &M = mats[i];
+            const int local = k - sp.first;
+            const int cls = M.cls;
+            if (cls == 0) {
+                vector_unit<4>(M, local, bad);
+            } else if (cls == 1) {
+                vector_unit<8>(M, local, bad);
+            } else if (cls == 2) {
+                vector_unit<16>(M, local, bad);
+            } else if (cls == 3) {
+                vector_unit<32>(M, local, bad);
+            } else if (cls == kBatchMergeClass) {
+                unsigned char *wsm = warp_smem();
+                merge_segment<ProdF64, AccF64, kBatchIpt>(
+                    local, M.n, M.rowptr, M.col, static_cast<const double *>(M.val), M.x, M.y,
+                    M.alpha, M.beta, M.tile_row, M.tile_nnz, M.carry_val, status,
+                    reinterpret_cast<double *>(wsm),
+                    reinterpret_cast<int *>(wsm + sizeof(double) * SEG), l2_evict_last(),
+                    l2_evict_first());
+            } else {  // kBatchTiledClass
+                int cur = 0;
+                if (pre_k == k)
+                    cur = pre_s;
+                else
+                    issue(M, local, 0);  // nothing is in flight here
+                pre_k = -1;
+                // start the next unit's copy if it is a tile unit of this claim
+                if (k + 1 < n) {
+                    int i2 = i;
+                    ClaimSpan s2 = sp;
+                    while (k + 1 >= s2.last) {
+                        ++i2;
+                        s2 = claim_span(unit0, i2, u0, n);
+                    }
+                    const BatchMat &M2 = mats[i2];
+                    if (M2.cls == kBatchTiledClass) {
+                        issue(M2, k + 1 - s2.first, cur ^ 1);
+                        pre_k = k + 1;
+                        pre_s = cur ^ 1;
+                    }
+                }
+                const int t0 = local * TG;
+                const int nt = M.tiles - t0 < TG ? M.tiles - t0 : TG;
+                // tile_seg of the unit's tiles (lane j: tile t0+j) and the
+                // row-start bit of the tile after the unit
+                const int tseg_l = lane < nt ? __ldg(M.tile_seg + t0 + lane) : 0;
+                const unsigned nb_last =
+                    t0 + nt < M.tiles
+                        ? (__ldg(reinterpret_cast<const unsigned *>(
+                               M.blob + (size_t)(t0 + nt) * TBB + kBit0)) & 1u)
+                        : 0u;
+                const bool ok = mbar_wait(bar0 + 8 * cur, (phases >> cur) & 1u);
+                phases ^= 1u << cur;
+                if (!ok) {
+                    timeout = 1;
+                    break;
+                }
+                const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
+                const unsigned char *tb = warp_smem() + cur * TG * TBB;
+                double xv[kBatchSigma], xn[kBatchSigma];
+                tile_gather<ProdF64, kBatchSigma>(t0, M.tiles, M.nnz, tb, M.x, keep, xv);
+#pragma unroll 1
+                for (int j = 0; j < nt; ++j) {
+                    const int t = t0 + j;
+                    const unsigned char *tj = tb + j * TBB;
+                    unsigned nb0 = nb_last;
+                    if (j + 1 < nt) {  // the next tile's x, in flight during this reduce
+                        nb0 = *reinterpret_cast<const unsigned *>(tj + TBB + kBit0) & 1u;
+                        tile_gather<ProdF64, kBatchSigma>(t + 1, M.tiles, M.nnz, tj + TBB, M.x,
+                                                          keep, xn);
+                    }
+                    const int tseg = __shfl_sync(0xffffffffu, tseg_l, j);
+                    tile_reduce<ProdF64, AccF64, kBatchSigma>(t, t == M.tiles - 1, tj, tseg, nb0,
+                                                              M.ne, xv, M.y, M.alpha, M.beta,
+                                                              M.carry_val, streaming, 0.0, 0.0,
+                                                              nullptr);
+#pragma unroll
+                    for (int q = 0; q < kBatchSigma; ++q) xv[q] = xn[q];
+                }
+                __syncwarp();  // every lane is done with the slot before it is refilled
+            }
+        }
+    }
+    if (timeout) {
+        // let a copy still in flight land (bounded) before the warp leaves
+        if (pre_k >= 0) mbar_wait(bar0 + 8 * pre_s, (phases >> pre_s) & 1u);
+        if (lane == 0) atomicOr(status, ST_TIMEOUT);
+    }
+    if (bad) atomicOr(status, ST_BAD_COL);
+}
+
+// The standalone fix-up (k_fixup.cu) and empty-row pass (k_tiled.cu) over
+// every merge/tiled matrix of the batch at once, with the same arithmetic:
+// blocks [0, short_blocks) take one global carry slot per thread (single
+// carries), the next n_runs blocks one multi-slot run each, the rest the empty
+// rows of tiled matrices.
+__global__ void __launch_bounds__(kFixupThreads)
+batch_fixup_kernel(const BatchMat *__restrict__ mats, BatchFix F, long long total_slots,
+                   int short_blocks)
+{
+    if (blockIdx.x < short_blocks) {
+        const long long g = (long long)blockIdx.x * kFixupThreads + threadIdx.x;
+        if (g >= total_slots) return;
+        const int k = find_matrix(F.tile0, F.nfix, g);
+        const BatchMat &M = mats[__ldg(F.mat + k)];
+        const int t = (int)(g - __ldg(F.tile0 + k)), T = M.tiles;
+        const int *crow = M.crow;
+        const int r = crow[t];
+        if (r >= M.m) return;
+        if ((t > 0 && crow[t - 1] == r) || (t + 1 < T && crow[t + 1] == r)) return;
+        fixup_single(M.y, r, M.alpha, M.carry_val[t]);
+        return;
+    }
+    const int j = blockIdx.x - short_blocks;
+    if (j < F.n_runs) {
+        __shared__ double s[kFixupThreads];
+        const BatchMat &M = mats[__ldg(F.run_mat + j)];
+        const int first = __ldg(F.run_first + j), len = __ldg(F.run_len + j);
+        s[threadIdx.x] = fixup_partial(M.carry_val, first, len, threadIdx.x);
+        __syncthreads();
+        for (int w = kFixupThreads / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) fixup_single(M.y, M.crow[first], M.alpha, s[0]);
+        return;
+    }
+    const long long e = (long long)(j - F.n_runs) * kFixupThreads + threadIdx.x;
+    if (e >= F.n_empty) return;
+    const BatchMat &M = mats[__ldg(F.empty_mat + e)];
+    double *yp = M.y + __ldg(F.empty_row + e);
+    *yp = M.beta == 0.0 ? 0.0 : M.beta * *yp;
+}
+
+}  // namespace
+
+int batch_max_ctas_per_sm()
+{
+    int blocks = 0;
+    cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_kernel, BT, kSmemBytes);
+    return blocks;
+}
+
+void launch_batch(const BatchMat *mats, int nmat, const long long *unit0, long long total,
+                  unsigned long long *queue, unsigned *status, int grid, cudaStream_t s)
+{
+    if (total > 0 && nmat > 0)
+        batch_kernel<<<grid, BT, kSmemBytes, s>>>(mats, nmat, unit0, total, queue, status);
+}
+
+void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total_slots,
+                        cudaStream_t s)
+{
+    if (total_slots <= 0 && F.n_empty <= 0) return;
+    const int short_blocks = (int)((total_slots + kFixupThreads - 1) / kFixupThreads);
+    const int empty_blocks = (F.n_empty + kFixupThreads - 1) / kFixupThreads;
+    batch_fixup_kernel<<<short_blocks + F.n_runs + empty_blocks, kFixupThreads, 0, s>>>(
+        mats, F, total_slots, short_blocks);
+}
+
+}  // namespace sbb

@@ -12,12 +12,13 @@
 // each and add its carries summed in a fixed order (per-thread strided sums,
 // then a shared-memory tree), so results are bit-reproducible.
 #include "../sbb_internal.h"
+#include "spmv_device.cuh"
 
 namespace sbb {
 
 namespace {
 
-constexpr int FT = 256;
+constexpr int FT = kFixupThreads;
 
 __global__ void runs_mark_kernel(const int *__restrict__ crow, int T, int m,
                                  int *__restrict__ run_first, int *__restrict__ run_len,
@@ -68,7 +69,7 @@ fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cva
         int r = crow[t];
         if (r >= m) return;
         if ((t > 0 && crow[t - 1] == r) || (t + 1 < T && crow[t + 1] == r)) return;
-        y[r] += alpha * cval[t];
+        fixup_single(y, r, alpha, cval[t]);
         return;
     }
     __shared__ double s[FT];
@@ -77,15 +78,13 @@ fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cva
     const int stride = dev_count ? (int)(gridDim.x - short_blocks) : n_runs;
     for (int j = blockIdx.x - short_blocks; j < n_runs; j += stride) {
         const int first = run_first[j], len = run_len[j];
-        double acc = 0.0;
-        for (int i = threadIdx.x; i < len; i += FT) acc += cval[first + i];
-        s[threadIdx.x] = acc;
+        s[threadIdx.x] = fixup_partial(cval, first, len, threadIdx.x);
         __syncthreads();
         for (int w = FT / 2; w > 0; w >>= 1) {
             if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
             __syncthreads();
         }
-        if (threadIdx.x == 0) y[crow[first]] += alpha * s[0];
+        if (threadIdx.x == 0) fixup_single(y, crow[first], alpha, s[0]);
         __syncthreads();
     }
 }

@@ -37,6 +37,7 @@
 
 #include "../sbb_internal.h"
 #include "common.cuh"
+#include "tiled_device.cuh"
 
 namespace sbb {
 
@@ -56,17 +57,6 @@ struct TiledPlan {
     double *carry_val = nullptr;
     CarryRuns runs;
 };
-
-__host__ __device__ constexpr size_t tile_bytes_of(int sigma, int vbytes)
-{
-    return (size_t)32 * sigma * (4 + vbytes) + 4 * (size_t)sigma;
-}
-// Per-warp staging of a tile's row sums: up to 32*sigma + 1 segments (only
-// tiles of sigma >= 8 stage them).
-__host__ __device__ constexpr size_t sum_bytes_of(int sigma)
-{
-    return sigma < 8 ? 0 : ((size_t)(32 * sigma + 1) * 8 + 127) / 128 * 128;
-}
 
 // Slot of nnz (lane, j) of group g inside a tile, for columns / FP32 values
 // and for FP64 values.
@@ -194,211 +184,6 @@ __global__ void empty_rows_kernel(const int *__restrict__ empty, int n_empty, do
         double *yp = y + empty[i];
         *yp = beta == 0.0 ? 0.0 : beta * *yp;
     }
-}
-
-// ---- TMA (1-D bulk async copy) helpers ------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ uint64_t evict_first_policy()
-{
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-// pol == 0: default L2 policy; otherwise an L2 cache-hint policy.
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar,
-                                         uint64_t pol)
-{
-    if (pol)
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-            " [%0], [%1], %2, [%3], %4;" ::"r"(dst),
-            "l"(src), "r"(bytes), "r"(bar), "l"(pol)
-            : "memory");
-    else
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
-            " [%0], [%1], %2, [%3];" ::"r"(dst),
-            "l"(src), "r"(bytes), "r"(bar)
-            : "memory");
-}
-// Bounded wait for the phase with the given parity; false if it never came
-// (the caller raises ST_TIMEOUT and stops instead of spinning for ever).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    for (int i = 0; i < (1 << 22); ++i) {
-        uint32_t ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-            " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
-// One tile from shared memory.
-// Columns in the blob were range-checked when the plan copied them, so x is
-// gathered without a per-element check; the final tile masks its padding.
-template <typename PT, int SIGMA>
-__device__ __forceinline__ void tile_gather(int t, int tiles, long long nnz, const unsigned char *tb,
-                                            const typename PT::V *__restrict__ x, uint64_t keep,
-                                            typename PT::V (&xv)[SIGMA])
-{
-    using V = typename PT::V;
-    constexpr int TILE = 32 * SIGMA;
-    const int lane = threadIdx.x & 31;
-    const int *s_col = reinterpret_cast<const int *>(tb);
-    const long long base = (long long)t * TILE;
-    const bool last = t == tiles - 1;
-#pragma unroll
-    for (int g = 0; g < SIGMA / 4; ++g) {
-        const int4 c = *reinterpret_cast<const int4 *>(s_col + g * 128 + lane * 4);
-        const int cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (last)
-                xv[g * 4 + j] = base + lane * SIGMA + g * 4 + j < nnz ? ld_keep(x + cc[j], keep) : V(0);
-            else
-                xv[g * 4 + j] = ld_keep(x + cc[j], keep);
-        }
-    }
-}
-
-// Reduces one tile whose x values are already gathered (xv).  Row sums are
-// staged in the warp's s_sum (index = segment - tseg) and written to y in one
-// coalesced pass at the end, so the divergent per-nnz loop touches no global
-// memory; ya/yb hold y of segments tseg+lane and tseg+32+lane, loaded when
-// the tile started.
-template <typename PT, typename ACC, int SIGMA>
-__device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned char *tb, int tseg,
-                                            unsigned next_bit0, const int *__restrict__ ne,
-                                            const typename PT::V (&xv)[SIGMA],
-                                            double *__restrict__ y, double alpha, double beta,
-                                            double *__restrict__ carry_val, uint64_t stream,
-                                            double ya, double yb, double *s_sum)
-{
-    using V = typename PT::V;
-    constexpr int TILE = 32 * SIGMA;
-    constexpr int G = SIGMA / 4;
-    const int lane = threadIdx.x & 31;
-    const V *s_val = reinterpret_cast<const V *>(tb + TILE * 4);
-    const unsigned *s_bits = reinterpret_cast<const unsigned *>(tb + TILE * (4 + sizeof(V)));
-
-    // this lane's sigma row-start bits
-    unsigned bits;
-    if constexpr (SIGMA == 32)
-        bits = s_bits[lane];
-    else
-        bits = (s_bits[(lane * SIGMA) >> 5] >> ((lane * SIGMA) & 31)) & ((1u << SIGMA) - 1u);
-
-    // 2. segment rows of this lane.  Tiles of sigma >= 8 stage row sums and
-    // write them in one coalesced pass; sigma = 4 tiles (few rows per lane,
-    // tightest register budget) write each row as it completes.
-    constexpr bool kStaged = SIGMA >= 8;
-    auto put = [&](int sg, double sum) {
-        if (kStaged)
-            s_sum[sg - tseg] = sum;
-        else
-            write_y(y + (ne ? __ldg(ne + sg) : sg), alpha, sum, beta, stream);
-    };
-    const unsigned b0 = __shfl_sync(0xffffffffu, bits, 0) & 1u;
-    const int cnt = __popc(bits);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int u = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += u;
-    }
-    const int head_seg = tseg - (int)b0 + incl - cnt;  // segment open before this lane's first nnz
-
-    // 3. products and lane-local segmented sums
-    ACC acc;
-    acc.zero();
-    double head = 0.0;
-    bool started = false;
-    int seg = head_seg;
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-        V v[4];
-        if constexpr (sizeof(V) == 8) {
-            double2 a = *reinterpret_cast<const double2 *>(s_val + g * 128 + lane * 2);
-            double2 b = *reinterpret_cast<const double2 *>(s_val + g * 128 + 64 + lane * 2);
-            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-        } else {
-            float4 a = *reinterpret_cast<const float4 *>(s_val + g * 128 + lane * 4);
-            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int s = g * 4 + j;
-            if ((bits >> s) & 1u) {
-                if (!started) {
-                    head = acc.get();
-                    started = true;
-                } else {  // a whole row inside this lane
-                    put(seg, acc.get());
-                }
-                acc.zero();
-                ++seg;
-            }
-            acc.add(PT::make(v[j], xv[s]));
-        }
-    }
-
-    // 4. warp segmented scan of lane carries, reset at lanes that start a row
-    double cv = acc.get();  // tail (or whole lane when no row starts here)
-    unsigned f = started;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        double vu = __shfl_up_sync(0xffffffffu, cv, o);
-        unsigned fu = __shfl_up_sync(0xffffffffu, f, o);
-        if (lane >= o) {
-            if (!f) cv += vu;
-            f |= fu;
-        }
-    }
-    double incoming = __shfl_up_sync(0xffffffffu, cv, 1);
-    if (lane == 0) incoming = 0.0;
-    // The row open when this lane began ends at its first row start.  For
-    // lane 0 with a start on its first nnz that row ended with the previous
-    // tile, which wrote it.
-    if (started && !(lane == 0 && b0)) put(head_seg, incoming + head);
-    const bool closes = last || next_bit0;  // the open row ends with this tile
-    if (lane == 31) {
-        if (closes) {
-            put(seg, cv);
-            carry_val[t] = 0.0;  // carry_row[t] == m
-        } else {
-            carry_val[t] = cv;   // carried into row_of(seg) == carry_row[t]
-        }
-    }
-    if (!kStaged) return;
-    // 5. rows completed here: segments tseg .. tseg+nwrite-1, coalesced
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int nwrite = total + (closes ? 1 : 0) - (int)b0;
-    __syncwarp();
-    for (int i = lane; i < nwrite; i += 32) {
-        double *yp = y + (ne ? __ldg(ne + tseg + i) : tseg + i);
-        double v = alpha * s_sum[i];
-        if (beta != 0.0) v += beta * (i < 32 ? ya : (i < 64 ? yb : ld_y(yp, stream)));
-        st_y(yp, v, stream);
-    }
-    __syncwarp();  // s_sum is reused by the next tile
 }
 
 // CTAs per SM the launch bounds aim at.
@@ -591,6 +376,15 @@ void launch_tiled_t(const TiledPlan &T, int m, int n, long long nnz, double alph
 }
 
 }  // namespace
+
+bool tiled_view(const Plan *p, TiledView *v)
+{
+    auto *T = static_cast<const TiledPlan *>(p->tiled);
+    if (!T) return false;
+    *v = TiledView{T->blob, T->tile_seg, T->ne, T->empty, T->carry_row, T->carry_val,
+                   T->tiles, T->sigma, T->n_empty, &T->runs};
+    return true;
+}
 
 // CSR5 sigma rule (include/anonymouslib_cuda.h:296-313), then rounded up to a
 // power of two in {4, 8, 16, 32} so a lane's row-start bits sit in one word.

@@ -1,11 +1,13 @@
 // k_vector.cu — K1: vector CSR SpMV, V lanes per row (V = 2..32).
 //
 // Replaces cusparseDcsrmv (SparseBLAS/src/dspmv_mgpu_v1.cu:200-204,
-// src/dspmv_mgpu_baseline.cu:163-167).  A group of V lanes owns one row, reads
-// its col/val with coalesced streaming loads (V consecutive nnz per step),
-// gathers x through the read-only path and reduces with warp shuffles
-// (xor butterfly: the order is fixed for a given V).  Good for regular
-// matrices whose row lengths are close to V; long rows serialise on one group.
+// src/dspmv_mgpu_baseline.cu:163-167).  A warp takes chunks of rows; in a
+// chunk a group of V lanes owns one row at a time, reads its col/val with
+// coalesced streaming loads (V consecutive nnz per step), gathers x through
+// the read-only path and reduces with warp shuffles (xor butterfly: the order
+// is fixed for a given V), with several rows' loads in flight per group
+// (vector_chunk).  Good for regular matrices whose row lengths are close to
+// V; long rows serialise on one group.
 #include "../sbb_internal.h"
 #include "common.cuh"
 #include "spmv_device.cuh"
@@ -16,22 +18,21 @@ namespace {
 
 constexpr int VT = 256;  // threads per CTA
 
+// Warp w of the grid takes chunks w, w + W, ... of CR rows (W = all warps).
 template <typename PT, typename ACC, int V>
 __global__ void __launch_bounds__(VT)
 vector_kernel(int m, int n, const int *__restrict__ rowptr, const int *__restrict__ col,
               const typename PT::V *__restrict__ val, const typename PT::V *__restrict__ x,
               double *__restrict__ y, double alpha, double beta, unsigned *status)
 {
-    const int group = (blockIdx.x * VT + threadIdx.x) / V;
-    const int groups = gridDim.x * (VT / V);
+    constexpr int CR = VectorShape<V>::CR;
+    static_assert(CR == vector_chunk_rows(V, V < 4 ? V : 4), "host and device chunk sizes differ");
+    const int warps = gridDim.x * (VT / 32);
+    const int chunks = (m + CR - 1) / CR;
+    const uint64_t stream = l2_evict_first();
     unsigned bad = 0;
-    // The trip count is uniform across the warp (all its groups step together)
-    // so the full-mask shuffles always see all 32 lanes.
-    const int warp_first = group - ((threadIdx.x & 31) / V);
-    for (int base = warp_first; base < m; base += groups) {
-        const int row = base + (group - warp_first);
-        vector_row<PT, ACC, V>(row, row < m, n, rowptr, col, val, x, y, alpha, beta, bad);
-    }
+    for (int c = blockIdx.x * (VT / 32) + (threadIdx.x >> 5); c < chunks; c += warps)
+        vector_chunk<PT, ACC, V>(c * CR, m, n, rowptr, col, val, x, y, alpha, beta, stream, bad);
     if (bad) atomicOr(status, ST_BAD_COL);
 }
 
@@ -44,7 +45,8 @@ void launch_vector_t(const CsrView &A, int V, double alpha, const typename PT::V
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    long long need = ((long long)A.m * V + VT - 1) / VT;
+    const int CR = vector_chunk_rows(V, V < 4 ? V : 4);  // VectorShape<V>::CR
+    long long need = ((long long)(A.m + CR - 1) / CR * 32 + VT - 1) / VT;  // a warp per chunk
     int grid = (int)(need < (long long)sms * 64 ? need : (long long)sms * 64);
 #define SBB_VL(W)                                                                     \
     case W:                                                                           \

@@ -11,42 +11,105 @@ namespace sbb {
 
 constexpr int kLongRow = 32;  // K2: rows longer than this in a segment are summed by the warp
 
-// One row per group of V lanes (K1).  All 32 lanes of the warp call this
-// together (inactive groups pass active = false) so the full-mask shuffles
-// see every lane; the reduction order is fixed for a given V.
-template <typename PT, typename ACC, int V>
-__device__ __forceinline__ void vector_row(int row, bool active, int n, const int *__restrict__ rowptr,
-                                           const int *__restrict__ col,
-                                           const typename PT::V *__restrict__ val,
-                                           const typename PT::V *__restrict__ x,
-                                           double *__restrict__ y, double alpha, double beta,
-                                           unsigned &bad)
+// K1 chunk shape: 32/V rows per sub-step, U sub-steps in flight together, at
+// most 32 rows (CR) per chunk.
+template <int V, int U_ = (V < 4 ? V : 4)> struct VectorShape {
+    static constexpr int RPW = 32 / V;
+    static constexpr int U = U_;
+    static constexpr int CR = RPW * U < 32 ? RPW * U : 32;
+};
+
+// K1: one chunk of CR consecutive rows [r0, r0 + CR) by one warp, V lanes per
+// row.  Lane l first loads rowptr[r0+l], rowptr[r0+l+1] and y[r0+l]
+// (coalesced, all in flight together).  Row q of the chunk is then reduced by
+// lane group q % (32/V) in sub-step q / (32/V); the U sub-steps run together,
+// their loads issued before any of them is summed, so a warp keeps U row
+// fetches per group in flight instead of one (U = UU changes only which loads
+// are in flight together, never a sum, so a caller picks it for its register
+// budget).  Per row the order of the sum is fixed for a given V: lane i of
+// the group adds the products of nnz lo+i, lo+i+V, lo+i+2V, ... in that order,
+// then the group's partial sums meet in an xor butterfly.  Lane l ends with
+// row r0+l's sum and writes y[r0+l] (one coalesced store per chunk).  All 32
+// lanes call this together (the shuffles use the full mask).
+template <typename PT, typename ACC, int V, int UU = (V < 4 ? V : 4)>
+__device__ __forceinline__ void vector_chunk(int r0, int m, int n, const int *__restrict__ rowptr,
+                                             const int *__restrict__ col,
+                                             const typename PT::V *__restrict__ val,
+                                             const typename PT::V *__restrict__ x,
+                                             double *__restrict__ y, double alpha, double beta,
+                                             uint64_t stream, unsigned &bad)
 {
-    const int lane = threadIdx.x & (V - 1);
-    int lo = 0, hi = 0;
-    if (active) {
-        lo = __ldg(rowptr + row);
-        hi = __ldg(rowptr + row + 1);
+    using S = VectorShape<V, UU>;
+    constexpr int RPW = S::RPW, U = S::U, CR = S::CR;
+    const int lane = threadIdx.x & 31, g = lane / V, li = lane & (V - 1);
+    const bool in = lane < CR && r0 + lane < m;
+    int rlo = 0, rhi = 0;
+    double yv = 0.0;
+    if (in) {
+        rlo = __ldg(rowptr + r0 + lane);
+        rhi = __ldg(rowptr + r0 + lane + 1);
+        if (beta != 0.0) yv = ld_y(y + r0 + lane, stream);
     }
-    ACC acc;
-    acc.zero();
-    int k = lo + lane;
-    // two independent loads in flight per lane
-    for (; k + V < hi; k += 2 * V) {
-        int c0 = ld_stream(col + k), c1 = ld_stream(col + k + V);
-        auto v0 = ld_stream(val + k), v1 = ld_stream(val + k + V);
-        auto x0 = gather_x(x, c0, n, bad), x1 = gather_x(x, c1, n, bad);
-        acc.add(PT::make(v0, x0));
-        acc.add(PT::make(v1, x1));
-    }
-    if (k < hi) acc.add(PT::make(ld_stream(val + k), gather_x(x, ld_stream(col + k), n, bad)));
-    double sum = acc.get();
+    double out = 0.0;
+#pragma unroll 1
+    for (int j0 = 0; j0 * RPW < CR; j0 += U) {
+        int k[U], hi[U];
+        ACC acc[U];
 #pragma unroll
-    for (int o = V / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, V);
-    if (active && lane == 0) {
-        double *yp = y + row;
-        __stcs(yp, axpby(alpha, sum, beta, yp));
+        for (int u = 0; u < U; ++u) {
+            const int q = (j0 + u) * RPW + g;
+            k[u] = __shfl_sync(0xffffffffu, rlo, q) + li;
+            hi[u] = __shfl_sync(0xffffffffu, rhi, q);
+            acc[u].zero();
+        }
+        for (;;) {
+            bool any = false;
+            int c[U];
+            typename PT::V v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (k[u] < hi[u]) {
+                    c[u] = ld_stream(col + k[u]);
+                    v[u] = ld_stream(val + k[u]);
+                    any = true;
+                }
+            }
+            if (!any) break;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (k[u] < hi[u]) {
+                    acc[u].add(PT::make(v[u], gather_x(x, c[u], n, bad)));
+                    k[u] += V;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            double sum = acc[u].get();
+#pragma unroll
+            for (int o = V / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, V);
+            // row q = (j0+u)*RPW + g lands in lane q
+            const double r = __shfl_sync(0xffffffffu, sum, (lane % RPW) * V);
+            if (lane / RPW == j0 + u) out = r;
+        }
     }
+    if (in) st_y(y + r0 + lane, beta == 0.0 ? alpha * out : alpha * out + beta * yv, stream);
+}
+
+// Carry fix-up arithmetic shared by the standalone fix-up (k_fixup.cu) and
+// the batch fix-up (k_batch.cu): a single carry is added as y[r] + alpha*c; a
+// run of carries is summed by kFixupThreads threads (thread i: slots i,
+// i + kFixupThreads, ... in order) and then by a shared-memory tree.
+constexpr int kFixupThreads = 256;
+__device__ __forceinline__ void fixup_single(double *y, int r, double alpha, double c)
+{
+    y[r] += alpha * c;
+}
+__device__ __forceinline__ double fixup_partial(const double *cval, int first, int len, int i)
+{
+    double acc = 0.0;
+    for (; i < len; i += kFixupThreads) acc += cval[first + i];
+    return acc;
 }
 
 __device__ __forceinline__ double warp_sum(double v)

@@ -94,6 +94,60 @@ void launch_merge_f32(const CsrView &A, int ipt, const MergeScratch &S,
                       unsigned *status, cudaStream_t s);
 int merge_max_ctas_per_sm(int ipt, bool f32);
 
+// ---- batched form (k_batch.cu) ----------------------------------------------
+constexpr int kBatchIpt = 6;        // merge-path class: items per lane (as its plain plan)
+constexpr int kBatchMergeClass = 4; // classes 0..3: vector CSR with V = 4 << cls
+constexpr int kBatchTiledClass = 5; // CSR5-style tiles, sigma = kBatchSigma
+constexpr int kBatchSigma = 4;
+constexpr int kBatchTileGroup = 4;  // tiled class: tiles per work unit (one bulk copy)
+constexpr int kBatchClaim = 16;     // work units a warp claims per queue access
+constexpr int kBatchVectorNnz = 1024; // vector classes: about this many nnz per work unit
+constexpr int kBatchVectorU = 2;    // vector classes: rows of a lane group in flight together
+// Rows per K1 chunk for V lanes per row and U rows in flight per lane group
+// (VectorShape<V, U>::CR in spmv_device.cuh).
+constexpr int vector_chunk_rows(int V, int U) { return (32 / V) * U < 32 ? (32 / V) * U : 32; }
+struct BatchMat {                   // one matrix of a batch, as the kernel sees it
+    const int *rowptr, *col;
+    const void *val;
+    const double *x;
+    double *y;
+    int m, n, cls;
+    int vsteps;                      // vector classes: chunks per unit
+    double alpha, beta;
+    const int *tile_row, *tile_nnz;  // merge class: segment coordinates
+    const int *crow;                 // merge/tiled: static carry row of each tile
+    double *carry_val;
+    int tiles;
+    long long nnz;
+    const unsigned char *blob;       // tiled class
+    const int *tile_seg, *ne;
+};
+// Flat view of every merge/tiled matrix's carries (and of the tiled
+// matrices' empty rows) for the batch fix-up.
+struct BatchFix {
+    const long long *tile0;          // nfix+1: first global carry slot of each matrix with slots
+    const int *mat;                  // nfix: batch index of each such matrix
+    int nfix;
+    const int *run_mat, *run_first, *run_len;  // multi-slot runs (all matrices)
+    int n_runs;
+    const int *empty_row, *empty_mat;          // empty rows of tiled matrices: y = beta*y
+    int n_empty;
+};
+// What the batch needs from a tiled plan.
+struct Plan;
+struct TiledView {
+    const unsigned char *blob;
+    const int *tile_seg, *ne, *empty, *carry_row;
+    double *carry_val;
+    int tiles, sigma, n_empty;
+    const CarryRuns *runs;
+};
+bool tiled_view(const Plan *p, TiledView *v);
+int batch_max_ctas_per_sm();
+void launch_batch(const BatchMat *mats, int nmat, const long long *unit0, long long total,
+                  unsigned long long *queue, unsigned *status, int grid, cudaStream_t s);
+void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total_slots,
+                        cudaStream_t s);
 
 // Boundary pieces (drop-in): sum of val*x over [lo, hi) per piece.
 void launch_pieces(const long long *lo, const long long *hi, int npieces,

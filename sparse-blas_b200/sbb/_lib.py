@@ -46,6 +46,13 @@ class GenParams(C.Structure):
                 ("p_empty", C.c_double), ("unit_values", C.c_int)]
 
 
+class BatchItem(C.Structure):
+    """sbb_batch_item (include/sbb_spmv.h)."""
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("nnz", C.c_int), ("rowptr", vp), ("col", vp),
+                ("val", vp), ("x", vp), ("y", vp), ("alpha", C.c_double), ("beta", C.c_double),
+                ("cls", C.c_int)]
+
+
 # Every symbol include/sbb_spmv.h declares, with its ctypes signature.
 SIGNATURES = {
     "spMV_mgpu_baseline": (C.c_int, [C.c_int, C.c_int, C.c_longlong, dp, vp, vp, vp, vp, dp, vp,
@@ -70,6 +77,15 @@ SIGNATURES = {
     "sbb_plan_info_get": (C.c_int, [vp, C.POINTER(PlanInfo)]),
     "sbb_plan_partition": (C.c_int, [vp, vp, vp, C.c_int]),
     "sbb_plan_destroy": (C.c_int, [vp]),
+    "sbb_batch_create": (C.c_int, [C.POINTER(vp), C.POINTER(BatchItem), C.c_int, vp]),
+    "sbb_batch_run": (C.c_int, [vp, vp]),
+    "sbb_batch_run_graph": (C.c_int, [vp, vp]),
+    "sbb_batch_run_each": (C.c_int, [vp, vp]),
+    "sbb_batch_launches": (C.c_int, [vp, C.c_int]),
+    "sbb_batch_check": (C.c_int, [vp]),
+    "sbb_batch_destroy": (C.c_int, [vp]),
+    "sbb_tune_classes": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double,
+                                   C.c_double, C.c_int, C.POINTER(C.c_float), vp]),
     "sbb_spmv_merge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_double, vp,
                                          C.c_double, vp, vp]),
     "sbb_last_error": (C.c_char_p, []),

@@ -83,3 +83,14 @@ def test_bad_arguments_rejected_before_any_device_work():
                             q=0) == -1
     bad_rp = np.array([0, 2], np.int64)  # rowptr[m] != nnz
     assert api.spMV_mgpu_baseline(1, 1, 1, 1.0, val, bad_rp, col, x, 0.0, y, ngpu=1) == -1
+
+
+def test_batch_and_tuner_reject_bad_arguments_on_the_host():
+    from sbb._lib import lib
+    assert lib().sbb_batch_create(None, None, 0, None) == -1
+    h = C.c_void_p()
+    assert lib().sbb_batch_create(C.byref(h), None, -1, None) == -1
+    assert lib().sbb_tune_classes(1, 1, 1, None, None, None, None, None, 1.0, 0.0, 3, None,
+                                  None) == -1
+    assert lib().sbb_batch_run(None, None) == -1
+    assert lib().sbb_batch_destroy(None) == 0
