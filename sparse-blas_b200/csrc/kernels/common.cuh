@@ -73,7 +73,7 @@ __device__ __forceinline__ T gather_x(const T *x, int c, int n, unsigned &bad)
 struct ProdF64 {
     using V = double;
     using P = double;
-    __device__ __forceinline__ static P make(double v, double xv) { return v * xv; }
+    __device__ __forceinline__ static P make(double v, double xv) { return __dmul_rn(v, xv); }
 };
 struct ProdF32 {
     using V = float;
@@ -92,7 +92,9 @@ struct ProdF32 {
 struct AccF64 {
     double s;
     __device__ __forceinline__ void zero() { s = 0.0; }
-    __device__ __forceinline__ void add(double p) { s += p; }
+    __device__ __forceinline__ void add(double p) { s = __dadd_rn(s, p); }
+    // s + v*x with one rounding (the vector and tiled kernels' step)
+    __device__ __forceinline__ void mac(double v, double x) { s = __fma_rn(v, x, s); }
     __device__ __forceinline__ double get() const { return s; }
 };
 struct AccF32 {
@@ -106,20 +108,28 @@ struct AccF32 {
         s = t;
         c = __fadd_rn(c, __fadd_rn(e, p.y));
     }
+    __device__ __forceinline__ void mac(float v, float x) { add(ProdF32::make(v, x)); }
     __device__ __forceinline__ double get() const { return (double)s + (double)c; }
 };
 
-// y update with the cuSPARSE convention: y is not read when beta == 0.
-__device__ __forceinline__ double axpby(double alpha, double sum, double beta,
-                                        const double *yp)
+// The y update alpha*sum + beta*y as fma(alpha, sum, beta*y); alpha*sum
+// alone when beta == 0 (y is then not read: the cuSPARSE convention).  The
+// FP64 arithmetic of every kernel is written with explicit-rounding
+// intrinsics (products __dmul_rn, sums __dadd_rn, multiply-adds and this
+// update __fma_rn),
+// which the compiler never fuses or splits, so the same data gives the same
+// bits in every kernel that runs a given reduction order (a standalone launch
+// and the batched launch in particular).
+__device__ __forceinline__ double y_update(double alpha, double sum, double beta, double yv)
 {
-    return beta == 0.0 ? alpha * sum : alpha * sum + beta * *yp;
+    return beta == 0.0 ? __dmul_rn(alpha, sum) : __fma_rn(alpha, sum, __dmul_rn(beta, yv));
 }
-// Same, with y read and written under a streaming L2 policy.
+// Same, with y read (only when beta != 0) and written under a streaming L2
+// policy.
 __device__ __forceinline__ void write_y(double *yp, double alpha, double sum, double beta,
                                         uint64_t pol)
 {
-    st_y(yp, beta == 0.0 ? alpha * sum : alpha * sum + beta * ld_y(yp, pol), pol);
+    st_y(yp, y_update(alpha, sum, beta, beta == 0.0 ? 0.0 : ld_y(yp, pol)), pol);
 }
 
 }  // namespace sbb

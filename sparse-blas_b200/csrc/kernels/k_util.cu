@@ -76,7 +76,7 @@ __global__ void pieces_kernel(const long long *__restrict__ lo, const long long 
     unsigned bad = 0;
     double sum = 0.0;
     for (long long k = lo[p] + threadIdx.x; k < hi[p]; k += 256)
-        sum += ld_stream(val + k) * gather_x(x, ld_stream(col + k), n, bad);
+        sum = __dadd_rn(sum, __dmul_rn(ld_stream(val + k), gather_x(x, ld_stream(col + k), n, bad)));
     s[threadIdx.x] = sum;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {

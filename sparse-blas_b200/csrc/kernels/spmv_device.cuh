@@ -78,7 +78,7 @@ __device__ __forceinline__ void vector_chunk(int r0, int m, int n, const int *__
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (k[u] < hi[u]) {
-                    acc[u].add(PT::make(v[u], gather_x(x, c[u], n, bad)));
+                    acc[u].mac(v[u], gather_x(x, c[u], n, bad));
                     k[u] += V;
                 }
             }
@@ -93,17 +93,17 @@ __device__ __forceinline__ void vector_chunk(int r0, int m, int n, const int *__
             if (lane / RPW == j0 + u) out = r;
         }
     }
-    if (in) st_y(y + r0 + lane, beta == 0.0 ? alpha * out : alpha * out + beta * yv, stream);
+    if (in) st_y(y + r0 + lane, y_update(alpha, out, beta, yv), stream);
 }
 
 // Carry fix-up arithmetic shared by the standalone fix-up (k_fixup.cu) and
-// the batch fix-up (k_batch.cu): a single carry is added as y[r] + alpha*c; a
+// the batch fix-up (k_batch.cu): a single carry is added as fma(alpha, c, y[r]); a
 // run of carries is summed by kFixupThreads threads (thread i: slots i,
 // i + kFixupThreads, ... in order) and then by a shared-memory tree.
 constexpr int kFixupThreads = 256;
 __device__ __forceinline__ void fixup_single(double *y, int r, double alpha, double c)
 {
-    y[r] += alpha * c;
+    y[r] = __fma_rn(alpha, c, y[r]);
 }
 __device__ __forceinline__ double fixup_partial(const double *cval, int first, int len, int i)
 {
@@ -209,8 +209,8 @@ __device__ __forceinline__ void merge_segment(
             acc.zero();
             for (int k = lo; k < hi; ++k) acc.add(s_p[k]);
             double *yp = y + r0 + i;
-            double v = alpha * acc.get();
-            if (beta != 0.0) v += beta * (b == 0 ? ypre : ld_y(yp, streaming));
+            const double v = y_update(alpha, acc.get(), beta,
+                                      beta == 0.0 ? 0.0 : (b == 0 ? ypre : ld_y(yp, streaming)));
             st_y(yp, v, streaming);
         }
         unsigned longs = __ballot_sync(0xffffffffu, i < nrows && is_long);
@@ -222,8 +222,8 @@ __device__ __forceinline__ void merge_segment(
             const double s = warp_range_sum<ACC>(s_p, llo, lhi, lane);
             if (lane == src) {
                 double *yp = y + r0 + i;
-                double v = alpha * s;
-                if (beta != 0.0) v += beta * (b == 0 ? ypre : ld_y(yp, streaming));
+                const double v = y_update(alpha, s, beta,
+                                          beta == 0.0 ? 0.0 : (b == 0 ? ypre : ld_y(yp, streaming)));
                 st_y(yp, v, streaming);
             }
         }

@@ -103,11 +103,12 @@ __device__ __forceinline__ void tile_gather(int t, int tiles, long long nnz, con
     }
 }
 
-// Reduces one tile whose x values are already gathered (xv).  Row sums are
-// staged in the warp's s_sum (index = segment - tseg) and written to y in one
-// coalesced pass at the end, so the divergent per-nnz loop touches no global
-// memory; ya/yb hold y of segments tseg+lane and tseg+32+lane, loaded when
-// the tile started.
+// Reduces one tile whose x values are already gathered (xv).  Tiles of
+// sigma >= 8 stage row sums in the warp's s_sum (index = segment - tseg) and
+// write them to y in one coalesced pass at the end, so the divergent per-nnz
+// loop touches no global memory; ya/yb hold y of segments tseg+lane and
+// tseg+32+lane, loaded when the tile started.  Tiles of sigma < 8 write each
+// row as it completes.
 template <typename PT, typename ACC, int SIGMA>
 __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned char *tb, int tseg,
                                             unsigned next_bit0, const int *__restrict__ ne,
@@ -135,10 +136,11 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
     // tightest register budget) write each row as it completes.
     constexpr bool kStaged = SIGMA >= 8;
     auto put = [&](int sg, double sum) {
-        if (kStaged)
+        if (kStaged) {
             s_sum[sg - tseg] = sum;
-        else
+        } else {
             write_y(y + (ne ? __ldg(ne + sg) : sg), alpha, sum, beta, stream);
+        }
     };
     const unsigned b0 = __shfl_sync(0xffffffffu, bits, 0) & 1u;
     const int cnt = __popc(bits);
@@ -180,7 +182,7 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
                 acc.zero();
                 ++seg;
             }
-            acc.add(PT::make(v[j], xv[s]));
+            acc.mac(v[j], xv[s]);
         }
     }
 
@@ -218,9 +220,8 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
     __syncwarp();
     for (int i = lane; i < nwrite; i += 32) {
         double *yp = y + (ne ? __ldg(ne + tseg + i) : tseg + i);
-        double v = alpha * s_sum[i];
-        if (beta != 0.0) v += beta * (i < 32 ? ya : (i < 64 ? yb : ld_y(yp, stream)));
-        st_y(yp, v, stream);
+        const double yv = beta == 0.0 ? 0.0 : (i < 32 ? ya : (i < 64 ? yb : ld_y(yp, stream)));
+        st_y(yp, y_update(alpha, s_sum[i], beta, yv), stream);
     }
     __syncwarp();  // s_sum is reused by the next tile
 }
