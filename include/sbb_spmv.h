@@ -137,7 +137,7 @@ int sbb_plan_info_get(sbb_plan_t plan, sbb_plan_info *info);
 int sbb_plan_partition(sbb_plan_t plan, int *h_row, int *h_nnz, int cap);
 int sbb_plan_destroy(sbb_plan_t plan);
 
-/* ---- batched form: many matrices, one persistent launch ----------------- */
+/* ---- batched form: many matrices, a few persistent launches -------------- */
 
 /* Kernel classes a matrix of a batch can use (the autotuner's and the
  * learned selector's choices; each computes the same SpMV):
@@ -164,11 +164,14 @@ typedef struct sbb_batch_s *sbb_batch_t;
  * The arrays must stay valid while the batch lives. */
 int sbb_batch_create(sbb_batch_t *batch, const sbb_batch_item *items, int count,
                      void *stream);
-/* All SpMVs of the batch in one persistent launch: warps take work units
- * (row chunks, merge segments or tile groups) from a device queue; one more
- * launch adds the carries of every merge/tiled matrix and finishes the empty
- * rows of tiled ones.  Each matrix's y is bit-identical to
- * sbb_batch_run_each with the same classes.  The y arrays must not overlap. */
+/* All SpMVs of the batch: one persistent kernel per kernel family present
+ * (vector classes 0..3, merge class 4, tiled class 5), each taking work units
+ * (row chunks, merge segments or tile groups) of all its matrices from its
+ * own device queue; the kernels run as parallel branches forked from `stream`
+ * and joined back, then one more launch adds the carries of every merge/tiled
+ * matrix and finishes the empty rows of tiled ones.  Each matrix's y is
+ * bit-identical to sbb_batch_run_each with the same classes.  The y arrays
+ * must not overlap. */
 int sbb_batch_run(sbb_batch_t batch, void *stream);
 /* Same launches, captured once in a CUDA graph and replayed. */
 int sbb_batch_run_graph(sbb_batch_t batch, void *stream);

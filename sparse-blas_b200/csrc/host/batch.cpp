@@ -1,5 +1,6 @@
-// batch.cpp — batched SpMV (one persistent launch, optionally a CUDA graph)
-// and the per-matrix class timer the autotuner uses.
+// batch.cpp — batched SpMV (one persistent kernel per kernel family, run as
+// parallel branches of the caller's stream or of one CUDA graph) and the
+// per-matrix class timer the autotuner uses.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,18 +14,25 @@ using namespace sbb;
 struct sbb_batch_s {
     std::vector<Plan *> plans;
     std::vector<BatchMat> host_mats;
-    BatchMat *d_mats = nullptr;
-    long long *d_unit0 = nullptr;
-    unsigned long long *d_queue = nullptr;  // [0]: next claim of kBatchClaim units
+    BatchMat *d_mats = nullptr;              // every matrix (the fix-up's view)
+    // per kernel family: its matrices, unit offsets, unit count, grid, bytes
+    BatchMat *d_fmats[kBatchFamilies] = {};
+    long long *d_unit0[kBatchFamilies] = {};
+    int fcount[kBatchFamilies] = {};
+    long long total[kBatchFamilies] = {};
+    int grid[kBatchFamilies] = {};
+    double fbytes[kBatchFamilies] = {};
+    unsigned long long *d_queue = nullptr;  // [f]: family f's next claim of kBatchClaim units
     unsigned *d_status = nullptr;
-    long long total = 0;
+    cudaStream_t side[kBatchFamilies - 1] = {};  // branches for the other families
+    cudaEvent_t ev_fork = nullptr, ev_join[kBatchFamilies - 1] = {};
     // carry fix-up of the merge/tiled-class matrices, empty rows of tiled ones
     BatchFix fix{};
     long long fix_slots = 0;
     long long *d_tile0 = nullptr;
     int *d_fix_mat = nullptr, *d_run_mat = nullptr, *d_run_first = nullptr, *d_run_len = nullptr;
     int *d_empty_row = nullptr, *d_empty_mat = nullptr;
-    int grid = 0, device = 0;
+    int device = 0;
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -52,11 +60,20 @@ static void batch_free(sbb_batch_s *b)
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->cap) cudaStreamDestroy(b->cap);
-    void *ptrs[] = {b->d_mats,    b->d_unit0,     b->d_queue,      b->d_status,
-                    b->d_tile0,   b->d_fix_mat,   b->d_run_mat,    b->d_run_first,
-                    b->d_run_len, b->d_empty_row, b->d_empty_mat};
+    for (int f = 0; f < kBatchFamilies - 1; f++) {
+        if (b->side[f]) cudaStreamDestroy(b->side[f]);
+        if (b->ev_join[f]) cudaEventDestroy(b->ev_join[f]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    void *ptrs[] = {b->d_mats,    b->d_queue,     b->d_status,    b->d_tile0,
+                    b->d_fix_mat, b->d_run_mat,   b->d_run_first, b->d_run_len,
+                    b->d_empty_row, b->d_empty_mat};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (int f = 0; f < kBatchFamilies; f++) {
+        if (b->d_fmats[f]) cudaFree(b->d_fmats[f]);
+        if (b->d_unit0[f]) cudaFree(b->d_unit0[f]);
+    }
     for (Plan *p : b->plans) {
         plan_free(p);
         delete p;
@@ -64,11 +81,33 @@ static void batch_free(sbb_batch_s *b)
     delete b;
 }
 
+// Families with work, largest (by bytes) first.
+static std::vector<int> active_families(const sbb_batch_s *b)
+{
+    std::vector<int> fams;
+    for (int f = 0; f < kBatchFamilies; f++)
+        if (b->total[f] > 0) fams.push_back(f);
+    std::stable_sort(fams.begin(), fams.end(),
+                     [&](int a, int c) { return b->fbytes[a] > b->fbytes[c]; });
+    return fams;
+}
+
+// The largest family's kernel runs on s, the others on side branches forked
+// from s and joined back before the fix-up (also inside a stream capture).
 static int enqueue(sbb_batch_s *b, cudaStream_t s)
 {
-    const int n = (int)b->host_mats.size();
-    SBB_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), s));
-    launch_batch(b->d_mats, n, b->d_unit0, b->total, b->d_queue, b->d_status, b->grid, s);
+    SBB_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long) * kBatchFamilies, s));
+    const std::vector<int> fams = active_families(b);
+    if (fams.size() > 1) SBB_CUDA(cudaEventRecord(b->ev_fork, s));
+    for (size_t j = 0; j < fams.size(); j++) {
+        const int f = fams[j];
+        cudaStream_t st = j == 0 ? s : b->side[j - 1];
+        if (j > 0) SBB_CUDA(cudaStreamWaitEvent(st, b->ev_fork, 0));
+        launch_batch(f, b->d_fmats[f], b->fcount[f], b->d_unit0[f], b->total[f], b->d_queue + f,
+                     b->d_status, b->grid[f], st);
+        if (j > 0) SBB_CUDA(cudaEventRecord(b->ev_join[j - 1], st));
+    }
+    for (size_t j = 1; j < fams.size(); j++) SBB_CUDA(cudaStreamWaitEvent(s, b->ev_join[j - 1], 0));
     launch_batch_fixup(b->d_mats, b->fix, b->fix_slots, s);
     SBB_CUDA(cudaGetLastError());
     return SBB_OK;
@@ -86,7 +125,9 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
     auto s = static_cast<cudaStream_t>(stream);
     auto *b = new sbb_batch_s();
     cudaGetDevice(&b->device);
-    std::vector<long long> unit0(count + 1, 0);
+    std::vector<BatchMat> fmats[kBatchFamilies];
+    std::vector<long long> funit0[kBatchFamilies];
+    for (auto &u : funit0) u.push_back(0);
     std::vector<long long> tile0(1, 0);
     std::vector<int> fix_mat, run_mat, run_first, run_len, empty_row, empty_mat;
     // copies cnt ints from the device; false (error set) on failure
@@ -196,9 +237,15 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
             units = (it.m + rows_per_unit - 1) / rows_per_unit;
         }
         b->host_mats.push_back(M);
-        unit0[i + 1] = unit0[i] + units;
+        const int f = batch_family(it.cls);
+        fmats[f].push_back(M);
+        funit0[f].push_back(funit0[f].back() + units);
+        b->fbytes[f] += 12.0 * it.nnz + 4.0 * (it.m + 1) + 8.0 * it.n + 16.0 * it.m;
     }
-    b->total = unit0[count];
+    for (int f = 0; f < kBatchFamilies; f++) {
+        b->fcount[f] = (int)fmats[f].size();
+        b->total[f] = funit0[f].back();
+    }
     auto fail = [&](cudaError_t e) {
         set_error(std::string("batch setup: ") + cudaGetErrorString(e));
         batch_free(b);
@@ -207,9 +254,23 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
     cudaError_t e;
     const int nfix = (int)fix_mat.size(), nruns = (int)run_mat.size();
     const int nempty = (int)empty_row.size();
-    if ((e = cudaMalloc(&b->d_mats, sizeof(BatchMat) * std::max(count, 1))) ||
-        (e = cudaMalloc(&b->d_unit0, sizeof(long long) * (count + 1))) ||
-        (e = cudaMalloc(&b->d_queue, sizeof(unsigned long long))) ||
+    for (int f = 0; f < kBatchFamilies; f++) {
+        const size_t nf = fmats[f].size();
+        if ((e = cudaMalloc(&b->d_fmats[f], sizeof(BatchMat) * std::max<size_t>(nf, 1))) ||
+            (e = cudaMalloc(&b->d_unit0[f], sizeof(long long) * (nf + 1))) ||
+            (nf && (e = cudaMemcpyAsync(b->d_fmats[f], fmats[f].data(), sizeof(BatchMat) * nf,
+                                        cudaMemcpyHostToDevice, s))) ||
+            (e = cudaMemcpyAsync(b->d_unit0[f], funit0[f].data(), sizeof(long long) * (nf + 1),
+                                 cudaMemcpyHostToDevice, s)))
+            return fail(e);
+    }
+    for (int f = 0; f < kBatchFamilies - 1; f++)
+        if ((e = cudaStreamCreateWithFlags(&b->side[f], cudaStreamNonBlocking)) ||
+            (e = cudaEventCreateWithFlags(&b->ev_join[f], cudaEventDisableTiming)))
+            return fail(e);
+    if ((e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) ||
+        (e = cudaMalloc(&b->d_mats, sizeof(BatchMat) * std::max(count, 1))) ||
+        (e = cudaMalloc(&b->d_queue, sizeof(unsigned long long) * kBatchFamilies)) ||
         (e = cudaMalloc(&b->d_status, sizeof(unsigned))) ||
         (e = cudaMalloc(&b->d_tile0, sizeof(long long) * (nfix + 1))) ||
         (e = cudaMalloc(&b->d_fix_mat, sizeof(int) * std::max(nfix, 1))) ||
@@ -230,7 +291,6 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
         (e = up(b->d_empty_row, empty_row.data(), sizeof(int) * nempty)) ||
         (e = up(b->d_empty_mat, empty_mat.data(), sizeof(int) * nempty)) ||
         (e = up(b->d_mats, b->host_mats.data(), sizeof(BatchMat) * count)) ||
-        (e = up(b->d_unit0, unit0.data(), sizeof(long long) * (count + 1))) ||
         (e = cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s)) ||
         (e = cudaStreamSynchronize(s)))
         return fail(e);
@@ -239,7 +299,8 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
     b->fix_slots = tile0.back();
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    b->grid = sms * std::max(batch_max_ctas_per_sm(), 1);
+    for (int f = 0; f < kBatchFamilies; f++)
+        b->grid[f] = sms * std::max(batch_max_ctas_per_sm(f), 1);
     *out = b;
     return SBB_OK;
 }
@@ -292,7 +353,7 @@ int sbb_batch_launches(sbb_batch_t b, int per_matrix)
 {
     if (!b) return 0;
     if (!per_matrix)
-        return (b->total > 0 ? 1 : 0) + (b->fix_slots > 0 || b->fix.n_empty > 0 ? 1 : 0);
+        return (int)active_families(b).size() + (b->fix_slots > 0 || b->fix.n_empty > 0 ? 1 : 0);
     int n = 0;
     for (Plan *p : b->plans) n += plan_launches(p);
     return n;

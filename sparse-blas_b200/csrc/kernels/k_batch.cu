@@ -1,29 +1,27 @@
-// k_batch.cu — many SpMVs of uneven sizes in one persistent launch.
+// k_batch.cu — many SpMVs of uneven sizes in a few persistent launches.
 //
 // The reference runs tasks from a host pool with an OpenMP thread per GPU
-// and q streams each (SparseBLAS/src/dspmv_mgpu_v2.cu:73-188).  Here the pool
-// is a device work queue: each matrix of the batch contributes work units -
-// row chunks for the vector-CSR classes, warp segments for the merge-path
-// class, groups of kBatchTileGroup tiles for the tiled class - and the warps
-// of one persistent grid claim kBatchClaim consecutive units per queue access
-// (one atomic on one counter) until the queue is empty.  A unit runs exactly
-// the device code the standalone kernel runs for it (spmv_device.cuh,
-// tiled_device.cuh), and the carries and empty rows of every merge/tiled
-// matrix are then finished by one fix-up launch with the standalone fix-up's
-// arithmetic, so every matrix's y is bit-identical to a standalone launch with
-// the same class.  A tiled unit is copied into shared memory with one TMA bulk
-// copy; while a warp reduces a unit, the copy of the next unit of its claim is
-// in flight, and the x values of each tile are gathered before the previous
-// tile is reduced.
+// and q streams each (SparseBLAS/src/dspmv_mgpu_v2.cu:73-188).  Here each
+// kernel family of the batch (vector-CSR classes, the merge-path class, the
+// tiled class) has one persistent kernel and one device work queue: every
+// matrix of the family contributes work units - row chunks, warp segments or
+// groups of kBatchTileGroup tiles - and the warps of the family's grid claim
+// kBatchClaim consecutive units per queue access (one atomic on one counter)
+// until the queue is empty.  The families' kernels run side by side (parallel
+// branches of one stream or graph); a kernel holds only its family's code, so
+// it gets the register budget and occupancy that code needs.  A unit runs
+// exactly the device code the standalone kernel runs for it
+// (spmv_device.cuh, tiled_device.cuh), and the carries and empty rows of every
+// merge/tiled matrix are then finished by one fix-up launch with the
+// standalone fix-up's arithmetic, so every matrix's y is bit-identical to a
+// standalone launch with the same class.  A tiled unit is copied into shared
+// memory with one TMA bulk copy; while a warp reduces a unit, the copy of the
+// next unit of its claim is in flight, and the x values of each tile are
+// gathered before the previous tile is reduced.
 #include "../sbb_internal.h"
 #include "common.cuh"
 #include "spmv_device.cuh"
 #include "tiled_device.cuh"
-
-// CTAs per SM the batch kernel's register budget aims at.
-#ifndef SBB_BATCH_MINB
-#define SBB_BATCH_MINB 2
-#endif
 
 namespace sbb {
 
@@ -35,18 +33,30 @@ constexpr int SEG = 32 * kBatchIpt;
 constexpr uint32_t TBB = (uint32_t)tile_bytes_of(kBatchSigma, 8);
 constexpr int TG = kBatchTileGroup;
 constexpr uint32_t kBit0 = 32 * kBatchSigma * 12;  // offset of a tile's row-start bits
-constexpr size_t kMergeWarpBytes = sizeof(double) * SEG + sizeof(int) * (SEG + 1);
-constexpr size_t kTiledWarpBytes = 2 * (size_t)TG * TBB;  // two unit slots
-// per-warp shared memory (dynamic): a merge segment's staging or two tile slots
-constexpr size_t kWarpBytes =
-    ((kMergeWarpBytes > kTiledWarpBytes ? kMergeWarpBytes : kTiledWarpBytes) + 127) / 128 * 128;
-constexpr size_t kSmemBytes = BW * kWarpBytes;
 static_assert(TBB % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-__device__ __forceinline__ unsigned char *warp_smem()
+// Per family: dynamic shared memory per warp (merge: a segment's staging;
+// tiled: two unit slots) and the CTAs per SM its register budget aims at.
+template <int FAM> struct FamShape;
+template <> struct FamShape<kFamVector> {
+    static constexpr size_t kWarpBytes = 0;
+    static constexpr int MINB = kBatchVectorU >= 4 ? 3 : 4;  // no spills at either
+};
+template <> struct FamShape<kFamMerge> {
+    static constexpr size_t kWarpBytes =
+        (sizeof(double) * SEG + sizeof(int) * (SEG + 1) + 127) / 128 * 128;
+    static constexpr int MINB = 4;
+};
+template <> struct FamShape<kFamTiled> {
+    static constexpr size_t kWarpBytes = 2 * (size_t)TG * TBB;
+    static constexpr int MINB = 3;  // 80 registers: the tile path does not spill
+};
+template <int FAM> constexpr size_t fam_smem() { return BW * FamShape<FAM>::kWarpBytes; }
+
+template <int FAM> __device__ __forceinline__ unsigned char *warp_smem()
 {
     extern __shared__ __align__(128) unsigned char s_dyn[];
-    return s_dyn + (size_t)(threadIdx.x >> 5) * kWarpBytes;
+    return s_dyn + (size_t)(threadIdx.x >> 5) * FamShape<FAM>::kWarpBytes;
 }
 
 // A vector-class unit: vsteps consecutive chunks of CR rows (kBatchVectorU
@@ -90,32 +100,31 @@ __device__ __forceinline__ ClaimSpan claim_span(const long long *unit0, int i, l
     return ClaimSpan{(int)a, (int)(b < n ? b : n)};
 }
 
-__global__ void __launch_bounds__(BT, SBB_BATCH_MINB)
+template <int FAM>
+__global__ void __launch_bounds__(BT, FamShape<FAM>::MINB)
 batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__restrict__ unit0,
              long long total, unsigned long long *queue, unsigned *status)
 {
-    __shared__ __align__(8) uint64_t bars[BW][2];
+    __shared__ __align__(8) uint64_t bars[FAM == kFamTiled ? BW : 1][2];
     const int lane = threadIdx.x & 31;
-    const uint32_t bar0 = smem_u32(&bars[threadIdx.x >> 5][0]);
-    if (lane == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar0 + 8, 1);
-        mbar_fence_init();
-    }
-    __syncwarp();
-    // Whole warp: copy the tiles of unit `unit` of MM into slot `sl`.  The
-    // slot may have been written by the merge staging (generic proxy) before:
-    // every lane fences its writes against the async proxy before lane 0
-    // starts the copy.
-    auto issue = [&](const BatchMat &MM, int unit, int sl) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    uint32_t bar0 = 0;
+    if constexpr (FAM == kFamTiled) {
+        bar0 = smem_u32(&bars[threadIdx.x >> 5][0]);
+        if (lane == 0) {
+            mbar_init(bar0, 1);
+            mbar_init(bar0 + 8, 1);
+            mbar_fence_init();
+        }
         __syncwarp();
+    }
+    // lane 0: copy the tiles of unit `unit` of MM into slot `sl`
+    auto issue = [&](const BatchMat &MM, int unit, int sl) {
         if (lane == 0) {
             const int t0 = unit * TG;
             const int nt = MM.tiles - t0 < TG ? MM.tiles - t0 : TG;
             const uint32_t bytes = (uint32_t)nt * TBB;
             mbar_expect_tx(bar0 + 8 * sl, bytes);
-            bulk_g2s(smem_u32(warp_smem() + sl * TG * TBB), MM.blob + (size_t)t0 * TBB, bytes,
+            bulk_g2s(smem_u32(warp_smem<FAM>() + sl * TG * TBB), MM.blob + (size_t)t0 * TBB, bytes,
                      bar0 + 8 * sl, evict_first_policy());
         }
     };
@@ -139,31 +148,32 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
             }
             const BatchMat &M = mats[i];
             const int local = k - sp.first;
-            const int cls = M.cls;
-            if (cls == 0) {
-                vector_unit<4>(M, local, bad);
-            } else if (cls == 1) {
-                vector_unit<8>(M, local, bad);
-            } else if (cls == 2) {
-                vector_unit<16>(M, local, bad);
-            } else if (cls == 3) {
-                vector_unit<32>(M, local, bad);
-            } else if (cls == kBatchMergeClass) {
-                unsigned char *wsm = warp_smem();
+            if constexpr (FAM == kFamVector) {
+                const int cls = M.cls;
+                if (cls == 0)
+                    vector_unit<4>(M, local, bad);
+                else if (cls == 1)
+                    vector_unit<8>(M, local, bad);
+                else if (cls == 2)
+                    vector_unit<16>(M, local, bad);
+                else
+                    vector_unit<32>(M, local, bad);
+            } else if constexpr (FAM == kFamMerge) {
+                unsigned char *wsm = warp_smem<FAM>();
                 merge_segment<ProdF64, AccF64, kBatchIpt>(
                     local, M.n, M.rowptr, M.col, static_cast<const double *>(M.val), M.x, M.y,
                     M.alpha, M.beta, M.tile_row, M.tile_nnz, M.carry_val, status,
                     reinterpret_cast<double *>(wsm),
                     reinterpret_cast<int *>(wsm + sizeof(double) * SEG), l2_evict_last(),
                     l2_evict_first());
-            } else {  // kBatchTiledClass
+            } else {
                 int cur = 0;
                 if (pre_k == k)
                     cur = pre_s;
                 else
                     issue(M, local, 0);  // nothing is in flight here
                 pre_k = -1;
-                // start the next unit's copy if it is a tile unit of this claim
+                // start the copy of the claim's next unit
                 if (k + 1 < n) {
                     int i2 = i;
                     ClaimSpan s2 = sp;
@@ -171,12 +181,9 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
                         ++i2;
                         s2 = claim_span(unit0, i2, u0, n);
                     }
-                    const BatchMat &M2 = mats[i2];
-                    if (M2.cls == kBatchTiledClass) {
-                        issue(M2, k + 1 - s2.first, cur ^ 1);
-                        pre_k = k + 1;
-                        pre_s = cur ^ 1;
-                    }
+                    issue(mats[i2], k + 1 - s2.first, cur ^ 1);
+                    pre_k = k + 1;
+                    pre_s = cur ^ 1;
                 }
                 const int t0 = local * TG;
                 const int nt = M.tiles - t0 < TG ? M.tiles - t0 : TG;
@@ -195,7 +202,7 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
                     break;
                 }
                 const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
-                const unsigned char *tb = warp_smem() + cur * TG * TBB;
+                const unsigned char *tb = warp_smem<FAM>() + cur * TG * TBB;
                 double xv[kBatchSigma], xn[kBatchSigma];
                 tile_gather<ProdF64, kBatchSigma>(t0, M.tiles, M.nnz, tb, M.x, keep, xv);
 #pragma unroll 1
@@ -220,10 +227,12 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
             }
         }
     }
-    if (timeout) {
-        // let a copy still in flight land (bounded) before the warp leaves
-        if (pre_k >= 0) mbar_wait(bar0 + 8 * pre_s, (phases >> pre_s) & 1u);
-        if (lane == 0) atomicOr(status, ST_TIMEOUT);
+    if constexpr (FAM == kFamTiled) {
+        if (timeout) {
+            // let a copy still in flight land (bounded) before the warp leaves
+            if (pre_k >= 0) mbar_wait(bar0 + 8 * pre_s, (phases >> pre_s) & 1u);
+            if (lane == 0) atomicOr(status, ST_TIMEOUT);
+        }
     }
     if (bad) atomicOr(status, ST_BAD_COL);
 }
@@ -273,20 +282,35 @@ batch_fixup_kernel(const BatchMat *__restrict__ mats, BatchFix F, long long tota
 
 }  // namespace
 
-int batch_max_ctas_per_sm()
+template <int FAM> static int max_ctas()
 {
     int blocks = 0;
-    cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kSmemBytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_kernel, BT, kSmemBytes);
+    cudaFuncSetAttribute(batch_kernel<FAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)fam_smem<FAM>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, batch_kernel<FAM>, BT, fam_smem<FAM>());
     return blocks;
 }
 
-void launch_batch(const BatchMat *mats, int nmat, const long long *unit0, long long total,
-                  unsigned long long *queue, unsigned *status, int grid, cudaStream_t s)
+int batch_max_ctas_per_sm(int fam)
 {
-    if (total > 0 && nmat > 0)
-        batch_kernel<<<grid, BT, kSmemBytes, s>>>(mats, nmat, unit0, total, queue, status);
+    return fam == kFamVector ? max_ctas<kFamVector>()
+                             : (fam == kFamMerge ? max_ctas<kFamMerge>() : max_ctas<kFamTiled>());
+}
+
+void launch_batch(int fam, const BatchMat *mats, int nmat, const long long *unit0,
+                  long long total, unsigned long long *queue, unsigned *status, int grid,
+                  cudaStream_t s)
+{
+    if (total <= 0 || nmat <= 0) return;
+    if (fam == kFamVector)
+        batch_kernel<kFamVector><<<grid, BT, fam_smem<kFamVector>(), s>>>(mats, nmat, unit0, total,
+                                                                          queue, status);
+    else if (fam == kFamMerge)
+        batch_kernel<kFamMerge><<<grid, BT, fam_smem<kFamMerge>(), s>>>(mats, nmat, unit0, total,
+                                                                        queue, status);
+    else
+        batch_kernel<kFamTiled><<<grid, BT, fam_smem<kFamTiled>(), s>>>(mats, nmat, unit0, total,
+                                                                        queue, status);
 }
 
 void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total_slots,

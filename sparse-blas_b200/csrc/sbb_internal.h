@@ -99,7 +99,7 @@ constexpr int kBatchIpt = 6;        // merge-path class: items per lane (as its 
 constexpr int kBatchMergeClass = 4; // classes 0..3: vector CSR with V = 4 << cls
 constexpr int kBatchTiledClass = 5; // CSR5-style tiles, sigma = kBatchSigma
 constexpr int kBatchSigma = 4;
-constexpr int kBatchTileGroup = 4;  // tiled class: tiles per work unit (one bulk copy)
+constexpr int kBatchTileGroup = 2;  // tiled class: tiles per work unit (one bulk copy)
 constexpr int kBatchClaim = 16;     // work units a warp claims per queue access
 constexpr int kBatchVectorNnz = 1024; // vector classes: about this many nnz per work unit
 constexpr int kBatchVectorU = 2;    // vector classes: rows of a lane group in flight together
@@ -143,9 +143,19 @@ struct TiledView {
     const CarryRuns *runs;
 };
 bool tiled_view(const Plan *p, TiledView *v);
-int batch_max_ctas_per_sm();
-void launch_batch(const BatchMat *mats, int nmat, const long long *unit0, long long total,
-                  unsigned long long *queue, unsigned *status, int grid, cudaStream_t s);
+// Kernel families of the batch: one persistent kernel each, compiled to its
+// own register budget (vector classes 0..3, the merge class, the tiled class).
+enum { kFamVector = 0, kFamMerge = 1, kFamTiled = 2, kBatchFamilies = 3 };
+inline int batch_family(int cls)
+{
+    return cls < kBatchMergeClass ? kFamVector : (cls == kBatchMergeClass ? kFamMerge : kFamTiled);
+}
+int batch_max_ctas_per_sm(int fam);
+// Units [0, total) of the family's matrices mats[0..nmat) (unit0: nmat+1
+// prefix offsets), claimed from *queue.
+void launch_batch(int fam, const BatchMat *mats, int nmat, const long long *unit0,
+                  long long total, unsigned long long *queue, unsigned *status, int grid,
+                  cudaStream_t s);
 void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total_slots,
                         cudaStream_t s);
 
