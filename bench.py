@@ -214,18 +214,9 @@ def run_reference(args, ws, rank):
 
 
 def default_class(A):
-    """The plain path's heuristic (default_kernel_choice in csrc/host/plan.cpp)
-    on the batch classes: vector CSR with V = next power of two >= mean row
-    length (4..32) when rows are short and even, the sigma = 4 tiles
-    otherwise."""
-    L = np.diff(A.rowptr)
-    mean = float(L.mean()) if len(L) else 0.0
-    v, cls = 4, 0
-    while v < 32 and v < mean:
-        v <<= 1
-        cls += 1
-    mx = int(L.max()) if len(L) else 0
-    return cls if (mx <= 4 * v and mx <= 128) else 5
+    """The plain path's heuristic on the batch classes (sbb.selector)."""
+    from sbb.selector import heuristic_class
+    return heuristic_class(A.rowptr)
 
 
 BATCH_METRIC = ("batched SpMV GB/s (FP64 CSR matrices; one CUDA graph: a persistent kernel per "
@@ -256,9 +247,11 @@ def c5_matrices(count, dev):
 def run_batch(args, ws, rank, local):
     """c5: 512 matrices; per-matrix plain launches vs one graph launch of the
     batch (a persistent kernel per kernel family, then the carry fix-up), with
-    the heuristic's and the exhaustive autotuner's classes."""
+    the learned selector's, the heuristic's and the exhaustive autotuner's
+    classes.  ``value`` is the batch with the selector's classes."""
     import torch
     from sbb.batch import Batch, tune
+    from sbb.selector import Selector
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     count = args.batch_count
@@ -271,6 +264,10 @@ def run_batch(args, ws, rank, local):
     t_tune = time.perf_counter() - t_tune
     best = [int(np.argmin(t)) for t in times]
     default = [default_class(d["A"]) for d in mats]
+    sel = Selector()
+    t_sel = time.perf_counter()
+    mlp = [sel.select(d) for d in mats]  # features, MLP and argmin on the GPU
+    t_sel = time.perf_counter() - t_sel
     stream = torch.cuda.current_stream()
 
     def timed(fn, reps):
@@ -287,7 +284,7 @@ def run_batch(args, ws, rank, local):
         return e0.elapsed_time(e1) / reps
 
     res = {}
-    for name, classes in (("default", default), ("tuned", best)):
+    for name, classes in (("mlp", mlp), ("default", default), ("tuned", best)):
         B = Batch(mats, classes)
         res[f"each_{name}_ms"] = timed(B.run_each, args.batch_reps)
         res[f"batch_{name}_ms"] = timed(B.run_graph, args.batch_reps)
@@ -297,7 +294,7 @@ def run_batch(args, ws, rank, local):
         B.close()
     best_sum = float(times.min(axis=1).sum())
     pick = lambda cls: float(sum(times[i, c] for i, c in enumerate(cls)))  # noqa: E731
-    ms = max_over_ranks(res["batch_tuned_ms"], ws)
+    ms = max_over_ranks(res["batch_mlp_ms"], ws)
     value = total_bytes * ws / (ms * 1e-3) / 1e9
     if rank != 0:
         return
@@ -308,14 +305,19 @@ def run_batch(args, ws, rank, local):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": C5_DESC.format(count=count),
                    "bytes_per_step": total_bytes, "l2_flush": "no (12.5 GB working set > L2)",
+                   "classes": "selector (MLP) choices; per-matrix launches of the "
+                              "heuristic's classes are the plain baseline",
                    "gen_s": round(t_gen, 1), "tune_s": round(t_tune, 1),
+                   "select_s": round(t_sel, 2),
+                   "classes_mlp": np.bincount(mlp, minlength=6).tolist(),
                    "classes_tuned": np.bincount(best, minlength=6).tolist(),
                    "classes_default": np.bincount(default, minlength=6).tolist(),
                    "speedup_batch_vs_each_default": round(res["each_default_ms"] / ms, 3),
-                   "speedup_batch_vs_each_tuned": round(res["each_tuned_ms"] / ms, 3),
+                   "speedup_batch_vs_each_mlp": round(res["each_mlp_ms"] / ms, 3),
+                   "regret_mlp": round(pick(mlp) / best_sum - 1, 4),
                    "regret_default": round(pick(default) / best_sum - 1, 4),
                    **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in res.items()}},
-        "gpu_launches": res["launches_batch_tuned"] * args.batch_reps,
+        "gpu_launches": res["launches_batch_mlp"] * args.batch_reps,
     }
     print(json.dumps(line), flush=True)
 

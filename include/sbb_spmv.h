@@ -190,6 +190,42 @@ int sbb_tune_classes(int m, int n, int nnz, const int *d_rowptr, const int *d_co
                      const double *d_val, const double *d_x, double *d_y, double alpha,
                      double beta, int reps, float *ms, void *stream);
 
+/* ---- learned class selector ---------------------------------------------- */
+
+/* A small FP32 MLP (12 features -> 64 -> 64 -> SBB_NUM_CLASSES, ReLU) that
+ * predicts, per kernel class, log2(t_class / t_best) of a plain launch; the
+ * selector picks the class with the smallest prediction.  No counterpart in
+ * the reference (its only tuner is the (ngpu, q) sweep of
+ * test/dspmv_test.cu:314-332).  The parameters are one float array of
+ * SBB_MLP_PARAMS entries: feature mean[12], feature std[12] (fixed input
+ * normalisation), W1[64][12], b1[64], W2[64][64], b2[64], W3[6][64], b3[6]. */
+#define SBB_MLP_FEATURES 12
+#define SBB_MLP_PARAMS 5406
+
+/* The 12 features of a device CSR matrix into d_feat (device, 12 floats):
+ * log2(1+m), log2(1+n), log2(1+nnz), log2(1+mean row length), coefficient of
+ * variation of the row lengths, log2(1+max row length), log2(1+max/mean),
+ * fraction of empty rows, of rows with <= 4 nnz, of rows with > 32 nnz,
+ * fraction of nnz in rows with > 128 nnz, mean column span of a row / n. */
+int sbb_features(int m, int n, int nnz, const int *d_rowptr, const int *d_col, float *d_feat,
+                 void *stream);
+/* d_y[N][6] = MLP(d_x[N][12]) (device arrays). */
+int sbb_mlp_forward(const float *d_params, const float *d_x, int N, float *d_y, void *stream);
+/* Loss L = sum_n w_n sum_c (y[n][c] - t[n][c])^2 / (6 * sum_n w_n) and its
+ * gradient d_grad[SBB_MLP_PARAMS] (zero for the normalisation entries);
+ * d_w may be NULL (all weights 1).  d_loss: one device float or NULL.  Sums
+ * over samples run in a fixed order (deterministic). */
+int sbb_mlp_grad(const float *d_params, const float *d_x, const float *d_t, const float *d_w,
+                 int N, float *d_grad, float *d_loss, void *stream);
+/* `steps` full-batch Adam steps (lr, L2 weight decay wd) on device, updating
+ * d_params in place; d_loss_hist (device, `steps` floats) or NULL. */
+int sbb_mlp_train(float *d_params, const float *d_x, const float *d_t, const float *d_w, int N,
+                  int steps, float lr, float wd, float *d_loss_hist, void *stream);
+/* Features, forward pass and argmin on the GPU for one device CSR matrix;
+ * *cls receives the chosen class (synchronises the stream). */
+int sbb_mlp_select(const float *d_params, int m, int n, int nnz, const int *d_rowptr,
+                   const int *d_col, int *cls, void *stream);
+
 /* Merge-path y = alpha*A*x + beta*y on device arrays that allocates nothing:
  * no counterpart in the reference.  For callers that must not call cudaMalloc
  * (a memory-capped or pre-partitioned process, a callback or real-time path

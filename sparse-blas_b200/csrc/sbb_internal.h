@@ -159,6 +159,24 @@ void launch_batch(int fam, const BatchMat *mats, int nmat, const long long *unit
 void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total_slots,
                         cudaStream_t s);
 
+// ---- learned class selector (k_mlp.cu) -------------------------------------
+constexpr int kMlpFeatures = 12, kMlpHidden = 64, kMlpClasses = SBB_NUM_CLASSES;
+constexpr int kMlpParams = 2 * kMlpFeatures + kMlpHidden * kMlpFeatures + kMlpHidden +
+                           kMlpHidden * kMlpHidden + kMlpHidden + kMlpClasses * kMlpHidden +
+                           kMlpClasses;
+// acc: 8 device words of scratch; feat: 12 floats (device).
+void launch_features(const int *rp, const int *col, int m, int n, long long nnz,
+                     unsigned long long *acc, float *feat, cudaStream_t s);
+void launch_mlp_forward(const float *P, const float *X, int N, float *Xn, float *H1, float *H2,
+                        float *Y, cudaStream_t s);
+void launch_mlp_backward(const float *P, int N, const float *Xn, const float *H1,
+                         const float *H2, const float *Y, const float *T, const float *W,
+                         float inv_norm, float *dY, float *dZ2, float *dZ1, float *G,
+                         float *loss, cudaStream_t s);
+void launch_mlp_adam(float *P, const float *G, float *M, float *V, int step, float lr, float wd,
+                     cudaStream_t s);
+void launch_mlp_argmin(const float *Y, int N, int *cls, cudaStream_t s);
+
 // Boundary pieces (drop-in): sum of val*x over [lo, hi) per piece.
 void launch_pieces(const long long *lo, const long long *hi, int npieces,
                    const int *col, const double *val, const double *x, int n,

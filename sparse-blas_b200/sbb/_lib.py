@@ -86,6 +86,11 @@ SIGNATURES = {
     "sbb_batch_destroy": (C.c_int, [vp]),
     "sbb_tune_classes": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_double,
                                    C.c_double, C.c_int, C.POINTER(C.c_float), vp]),
+    "sbb_features": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]),
+    "sbb_mlp_forward": (C.c_int, [vp, vp, C.c_int, vp, vp]),
+    "sbb_mlp_grad": (C.c_int, [vp, vp, vp, vp, C.c_int, vp, vp, vp]),
+    "sbb_mlp_train": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, vp]),
+    "sbb_mlp_select": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_int), vp]),
     "sbb_spmv_merge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_double, vp,
                                          C.c_double, vp, vp]),
     "sbb_last_error": (C.c_char_p, []),
