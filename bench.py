@@ -359,6 +359,96 @@ def run_reference_batch(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_f32(args, ws, rank, local):
+    """FP32-storage compensated form vs the FP64 plan on the same matrix, both
+    timed here (main kernel with CUDA events, whole steps), with max and
+    median per-row error against the FP64 double-double oracle."""
+    import ctypes as C
+    import torch
+    from sbb._lib import lib
+    from sbb.device import Plan
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    A, x_h, y_h, alpha, beta, desc = make_workload(args.workload)
+    m, n, nnz = A.m, A.n, A.nnz
+    bytes64 = algo_bytes(m, n, nnz)
+    bytes32 = 8 * nnz + 4 * (m + 1) + 4 * n + 16 * m
+    rp = torch.from_numpy(A.rowptr32()).to(dev)
+    col = torch.from_numpy(A.col).to(dev)
+    y0 = torch.from_numpy(y_h).to(dev)
+    kw = dict(tile_sigma=args.sigma) if args.kernel == "tiled" else {}
+    P64 = Plan(rp, col, torch.from_numpy(A.val).to(dev), n, kernel=args.kernel, **kw)
+    P32 = Plan(rp, col, torch.from_numpy(A.val.astype(np.float32)).to(dev), n, kernel=args.kernel,
+               f32=True, **kw)
+    x64 = torch.from_numpy(x_h).to(dev)
+    x32 = torch.from_numpy(x_h.astype(np.float32)).to(dev)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def timed(P, x, steps):
+        y = y0.clone()
+        for _ in range(args.warmup):
+            P.spmv(x, y, alpha, beta)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps + 2)]
+        for e in ev:
+            e.record(stream)
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for i in range(steps):
+            assert lib().sbb_spmv_timed(P.h, alpha, C.c_void_p(x.data_ptr()), beta,
+                                        C.c_void_p(y.data_ptr()), sp,
+                                        C.c_void_p(ev[2 + 2 * i].cuda_event),
+                                        C.c_void_p(ev[3 + 2 * i].cuda_event)) == 0
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        P.check()
+        kern = statistics.mean(ev[2 + 2 * i].elapsed_time(ev[3 + 2 * i]) for i in range(steps))
+        return ev[0].elapsed_time(ev[1]) / steps, kern
+
+    with ClockSampler(local) as clk:
+        step64, kern64 = timed(P64, x64, args.steps)
+        step32, kern32 = timed(P32, x32, args.steps)
+    ms32 = max_over_ranks(step32, ws)
+    y = y0.clone()
+    P32.spmv(x32, y, alpha, beta)
+    torch.cuda.synchronize()
+    got = y.cpu().numpy()
+    ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x_h, alpha, beta, y_h)
+    err = np.abs(got - ref) / np.where(sc > 0, sc, 1.0)
+    tag = {1: "vector_kernel", 2: "merge_kernel", 3: "tiled_kernel"}[P32.info()["kernel"]]
+    peak, peak_kind = peaks()
+    if rank == 0:
+        ach = bytes32 / (kern32 * 1e-3) / 1e9
+        print(json.dumps({
+            "metric": "SpMV GB/s, FP32-storage compensated form (algorithmic bytes "
+                      "8*nnz+4*(m+1)+4*n+16*m)",
+            "value": round(ws * bytes32 / (ms32 * 1e-3) / 1e9, 3), "unit": "GB/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": desc + " (val and x rounded to FP32, y FP64)", "m": m, "n": n,
+                       "nnz": nnz, "kernel": tag, "plan": {k: P32.info()[k] for k in
+                                                           ("tile_sigma", "vector_width",
+                                                            "items_per_thread")},
+                       "fp64_plan_ms_per_step": round(step64, 5),
+                       "fp64_kernel_ms": round(kern64, 5), "f32_kernel_ms": round(kern32, 5),
+                       "speedup_step_vs_fp64": round(step64 / step32, 3),
+                       "speedup_kernel_vs_fp64": round(kern64 / kern32, 3),
+                       "byte_ratio": round(bytes64 / bytes32, 3),
+                       "err_max": float(err.max()), "err_median": float(np.median(err)),
+                       "err_metric": "|y - y_oracle| / (|alpha| sum|a x| + |beta y|), FP64 "
+                                     "double-double oracle on the FP64 inputs"},
+            "roofline": {"bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(ach / peak, 4), "traffic": None, "peak_source": peak_kind},
+            "gpu_launches": lib().sbb_plan_launches(P32.h) * args.steps,
+            "clocks": clk.summary()}), flush=True)
+    P64.close()
+    P32.close()
+
+
 def run_sbb(args, ws, rank, local):
     import ctypes as C
     import torch
@@ -502,6 +592,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--f32", action="store_true",
+                    help="time the FP32-storage compensated form against the FP64 plan")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -511,6 +603,8 @@ def main():
             (run_reference_batch if args.workload == "c5" else run_reference)(args, ws, rank)
         elif args.workload == "c5":
             run_batch(args, ws, rank, local)
+        elif args.f32:
+            run_f32(args, ws, rank, local)
         else:
             run_sbb(args, ws, rank, local)
     finally:

@@ -108,9 +108,12 @@ typedef struct {
 int sbb_plan_create(sbb_plan_t *plan, int m, int n, int nnz,
                     const int *d_rowptr, const int *d_col, const double *d_val,
                     const sbb_config *cfg, void *stream);
-/* FP32-storage form: values (and x at run time) stored as float, each row
- * segment accumulated in FP32 with compensated (TwoSum) summation, segment
- * carries combined and alpha/beta applied in FP64. */
+/* FP32-storage form: values (and x at run time) stored as float, halving
+ * their bytes.  Each product of two floats is formed exactly in FP64 and the
+ * row segments, carries and alpha/beta update are FP64, so the result differs
+ * from the FP64 product of the rounded inputs only by FP64 summation error;
+ * against the FP64 inputs the error is that of rounding val and x to float
+ * (per row, about 1e-7 of sum_j |a_ij x_j|). */
 int sbb_plan_create_f32(sbb_plan_t *plan, int m, int n, int nnz,
                         const int *d_rowptr, const int *d_col,
                         const float *d_val, const sbb_config *cfg, void *stream);

@@ -67,9 +67,9 @@ __device__ __forceinline__ T gather_x(const T *x, int c, int n, unsigned &bad)
 }
 
 // Per-value products for the two storage forms.
-//   FP64: the product itself.
-//   FP32: (p, e) with p = fl(v*x) and e its exact rounding error (fmaf), the
-//         input to the compensated row-segment sum.
+//   FP64: the product itself, rounded.
+//   FP32 storage: the product of two floats taken in FP64, where it is exact
+//         (24 + 24 significand bits fit in 53).
 struct ProdF64 {
     using V = double;
     using P = double;
@@ -77,18 +77,19 @@ struct ProdF64 {
 };
 struct ProdF32 {
     using V = float;
-    using P = float2;
+    using P = double;
     __device__ __forceinline__ static P make(float v, float xv)
     {
-        float p = __fmul_rn(v, xv);
-        float e = __fmaf_rn(v, xv, -p);
-        return make_float2(p, e);
+        return __dmul_rn((double)v, (double)xv);  // exact
     }
 };
 
-// Running row-segment sums.  FP64: plain sum.  FP32: Knuth TwoSum with the
-// product errors folded into the compensation term; the segment value is
-// taken to FP64 as s + c.
+// Running row-segment sums, in FP64 for both storage forms.  For FP32
+// storage every product is exact, so the only rounding in a segment sum is
+// that of the FP64 additions: the form is compensated by construction, to
+// far below FP32's own rounding (a TwoSum-compensated FP32 sum would cost a
+// chain of about ten dependent FP32 operations per nnz, and that chain, not
+// the bytes, bounded the kernel's speed on B200).
 struct AccF64 {
     double s;
     __device__ __forceinline__ void zero() { s = 0.0; }
@@ -98,18 +99,12 @@ struct AccF64 {
     __device__ __forceinline__ double get() const { return s; }
 };
 struct AccF32 {
-    float s, c;
-    __device__ __forceinline__ void zero() { s = 0.f; c = 0.f; }
-    __device__ __forceinline__ void add(float2 p)
-    {
-        float t = __fadd_rn(s, p.x);
-        float bb = __fsub_rn(t, s);
-        float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(p.x, bb));
-        s = t;
-        c = __fadd_rn(c, __fadd_rn(e, p.y));
-    }
-    __device__ __forceinline__ void mac(float v, float x) { add(ProdF32::make(v, x)); }
-    __device__ __forceinline__ double get() const { return (double)s + (double)c; }
+    double s;
+    __device__ __forceinline__ void zero() { s = 0.0; }
+    __device__ __forceinline__ void add(double p) { s = __dadd_rn(s, p); }
+    // s + v*x with one rounding; v*x is exact in FP64, so this rounds once
+    __device__ __forceinline__ void mac(float v, float x) { s = __fma_rn((double)v, (double)x, s); }
+    __device__ __forceinline__ double get() const { return s; }
 };
 
 // The y update alpha*sum + beta*y as fma(alpha, sum, beta*y); alpha*sum
