@@ -168,7 +168,8 @@ typedef struct sbb_batch_s *sbb_batch_t;
 int sbb_batch_create(sbb_batch_t *batch, const sbb_batch_item *items, int count,
                      void *stream);
 /* All SpMVs of the batch: one persistent kernel per kernel family present
- * (vector classes 0..3, merge class 4, tiled class 5), each taking work units
+ * (vector classes 0-1, vector classes 2-3, merge class 4, tiled class 5),
+ * each taking work units
  * (row chunks, merge segments or tile groups) of all its matrices from its
  * own device queue; the kernels run as parallel branches forked from `stream`
  * and joined back, then one more launch adds the carries of every merge/tiled

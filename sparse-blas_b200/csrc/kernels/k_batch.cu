@@ -35,12 +35,12 @@ constexpr int TG = kBatchTileGroup;
 constexpr uint32_t kBit0 = 32 * kBatchSigma * 12;  // offset of a tile's row-start bits
 static_assert(TBB % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-// Per family: dynamic shared memory per warp (merge: a segment's staging;
-// tiled: two unit slots) and the CTAs per SM its register budget aims at.
-template <int FAM> struct FamShape;
-template <> struct FamShape<kFamVector> {
+// Per class kernel: dynamic shared memory per warp (merge: a segment's
+// staging; tiled: two unit slots) and the CTAs per SM its register budget
+// aims at (no spills at any of them).
+template <int FAM> struct FamShape {  // vector families
     static constexpr size_t kWarpBytes = 0;
-    static constexpr int MINB = kBatchVectorU >= 4 ? 3 : 4;  // no spills at either
+    static constexpr int MINB = 4;
 };
 template <> struct FamShape<kFamMerge> {
     static constexpr size_t kWarpBytes =
@@ -105,10 +105,11 @@ __global__ void __launch_bounds__(BT, FamShape<FAM>::MINB)
 batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__restrict__ unit0,
              long long total, unsigned long long *queue, unsigned *status)
 {
-    __shared__ __align__(8) uint64_t bars[FAM == kFamTiled ? BW : 1][2];
+    constexpr bool kTiled = FAM == kFamTiled;
+    __shared__ __align__(8) uint64_t bars[kTiled ? BW : 1][2];
     const int lane = threadIdx.x & 31;
     uint32_t bar0 = 0;
-    if constexpr (FAM == kFamTiled) {
+    if constexpr (kTiled) {
         bar0 = smem_u32(&bars[threadIdx.x >> 5][0]);
         if (lane == 0) {
             mbar_init(bar0, 1);
@@ -148,13 +149,13 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
             }
             const BatchMat &M = mats[i];
             const int local = k - sp.first;
-            if constexpr (FAM == kFamVector) {
-                const int cls = M.cls;
-                if (cls == 0)
+            if constexpr (FAM == kFamVectorNarrow) {
+                if (M.cls == 0)
                     vector_unit<4>(M, local, bad);
-                else if (cls == 1)
+                else
                     vector_unit<8>(M, local, bad);
-                else if (cls == 2)
+            } else if constexpr (FAM == kFamVectorWide) {
+                if (M.cls == 2)
                     vector_unit<16>(M, local, bad);
                 else
                     vector_unit<32>(M, local, bad);
@@ -227,7 +228,7 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
             }
         }
     }
-    if constexpr (FAM == kFamTiled) {
+    if constexpr (kTiled) {
         if (timeout) {
             // let a copy still in flight land (bounded) before the warp leaves
             if (pre_k >= 0) mbar_wait(bar0 + 8 * pre_s, (phases >> pre_s) & 1u);
@@ -293,8 +294,19 @@ template <int FAM> static int max_ctas()
 
 int batch_max_ctas_per_sm(int fam)
 {
-    return fam == kFamVector ? max_ctas<kFamVector>()
-                             : (fam == kFamMerge ? max_ctas<kFamMerge>() : max_ctas<kFamTiled>());
+    switch (fam) {
+    case 0: return max_ctas<0>();
+    case 1: return max_ctas<1>();
+    case 2: return max_ctas<2>();
+    default: return max_ctas<3>();
+    }
+}
+
+template <int FAM>
+static void launch_fam(const BatchMat *mats, int nmat, const long long *unit0, long long total,
+                       unsigned long long *queue, unsigned *status, int grid, cudaStream_t s)
+{
+    batch_kernel<FAM><<<grid, BT, fam_smem<FAM>(), s>>>(mats, nmat, unit0, total, queue, status);
 }
 
 void launch_batch(int fam, const BatchMat *mats, int nmat, const long long *unit0,
@@ -302,15 +314,12 @@ void launch_batch(int fam, const BatchMat *mats, int nmat, const long long *unit
                   cudaStream_t s)
 {
     if (total <= 0 || nmat <= 0) return;
-    if (fam == kFamVector)
-        batch_kernel<kFamVector><<<grid, BT, fam_smem<kFamVector>(), s>>>(mats, nmat, unit0, total,
-                                                                          queue, status);
-    else if (fam == kFamMerge)
-        batch_kernel<kFamMerge><<<grid, BT, fam_smem<kFamMerge>(), s>>>(mats, nmat, unit0, total,
-                                                                        queue, status);
-    else
-        batch_kernel<kFamTiled><<<grid, BT, fam_smem<kFamTiled>(), s>>>(mats, nmat, unit0, total,
-                                                                        queue, status);
+    switch (fam) {
+    case 0: launch_fam<0>(mats, nmat, unit0, total, queue, status, grid, s); break;
+    case 1: launch_fam<1>(mats, nmat, unit0, total, queue, status, grid, s); break;
+    case 2: launch_fam<2>(mats, nmat, unit0, total, queue, status, grid, s); break;
+    default: launch_fam<3>(mats, nmat, unit0, total, queue, status, grid, s); break;
+    }
 }
 
 void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total_slots,

@@ -102,7 +102,7 @@ constexpr int kBatchSigma = 4;
 constexpr int kBatchTileGroup = 2;  // tiled class: tiles per work unit (one bulk copy)
 constexpr int kBatchClaim = 16;     // work units a warp claims per queue access
 constexpr int kBatchVectorNnz = 1024; // vector classes: about this many nnz per work unit
-constexpr int kBatchVectorU = 2;    // vector classes: rows of a lane group in flight together
+constexpr int kBatchVectorU = 4;    // vector classes: rows of a lane group in flight together
 // Rows per K1 chunk for V lanes per row and U rows in flight per lane group
 // (VectorShape<V, U>::CR in spmv_device.cuh).
 constexpr int vector_chunk_rows(int V, int U) { return (32 / V) * U < 32 ? (32 / V) * U : 32; }
@@ -143,12 +143,16 @@ struct TiledView {
     const CarryRuns *runs;
 };
 bool tiled_view(const Plan *p, TiledView *v);
-// Kernel families of the batch: one persistent kernel each, compiled to its
-// own register budget (vector classes 0..3, the merge class, the tiled class).
-enum { kFamVector = 0, kFamMerge = 1, kFamTiled = 2, kBatchFamilies = 3 };
+// Kernel families of the batch: one persistent kernel each, compiled with
+// only its family's code (so with that code's register budget): vector CSR
+// with 4 or 8 lanes, with 16 or 32 lanes, the merge class, the tiled class.
+enum { kFamVectorNarrow = 0, kFamVectorWide = 1, kFamMerge = 2, kFamTiled = 3,
+       kBatchFamilies = 4 };
 inline int batch_family(int cls)
 {
-    return cls < kBatchMergeClass ? kFamVector : (cls == kBatchMergeClass ? kFamMerge : kFamTiled);
+    return cls < 2 ? kFamVectorNarrow
+                   : (cls < kBatchMergeClass ? kFamVectorWide
+                                             : (cls == kBatchMergeClass ? kFamMerge : kFamTiled));
 }
 int batch_max_ctas_per_sm(int fam);
 // Units [0, total) of the family's matrices mats[0..nmat) (unit0: nmat+1
