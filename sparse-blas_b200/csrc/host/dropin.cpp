@@ -125,9 +125,9 @@ enum class Merge { V1, V2, NONE };
 
 // Per-thread stream; device memory comes from the device's default pool,
 // which keeps freed blocks for the next call.
-cudaStream_t call_stream(int dev)
+cudaStream_t call_stream(int dev, int which = 0)
 {
-    static thread_local cudaStream_t s[64] = {};
+    static thread_local cudaStream_t s[2][64] = {};
     static thread_local bool pool_set[64] = {};
     if (dev < 0 || dev >= 64) return 0;
     if (!pool_set[dev]) {
@@ -138,8 +138,8 @@ cudaStream_t call_stream(int dev)
         }
         pool_set[dev] = true;
     }
-    if (!s[dev]) cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking);
-    return s[dev];
+    if (!s[which][dev]) cudaStreamCreateWithFlags(&s[which][dev], cudaStreamNonBlocking);
+    return s[which][dev];
 }
 
 // A few pinned words per thread, so the status read-back is truly
@@ -207,12 +207,12 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     // Special rows: slice extent != CSR extent, or split.
     std::vector<Piece> pieces;
     std::vector<int> first_piece(sl.size(), -1), last_piece(sl.size(), -1);
-    std::vector<char> covered(hr1 - hr0 + 1, 0);
+    std::vector<std::pair<int, int>> spans;  // covered row ranges [start_row, end_row]
     for (size_t t = 0; t < sl.size(); t++) {
         Slice &s = sl[t];
         int dev_m = s.end_row - s.start_row + 1;
         if (dev_m <= 0) continue;
-        std::fill(covered.begin() + (s.start_row - hr0), covered.begin() + (s.end_row - hr0 + 1), 1);
+        spans.push_back({s.start_row, s.end_row});
         long long lo = s.start_idx;
         long long hi = dev_m == 1 ? s.end_idx + 1 : rp[s.start_row + 1];
         if (s.start_flag || (dev_m == 1 && s.end_flag) || lo != rp[s.start_row] ||
@@ -230,10 +230,16 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         }
     }
 
-    // Input y of every row the host will rewrite after the copy back.
+    // Input y of every row the host will rewrite after the copy back: the
+    // rows of the hull in the gaps between covered ranges (found from the
+    // sorted ranges, not row by row), and the special rows.
     std::vector<std::pair<int, double>> saved;
-    for (int r = hr0; r <= hr1; r++)
-        if (!covered[r - hr0]) saved.push_back({r, y[r]});
+    std::sort(spans.begin(), spans.end());
+    int next = hr0;  // first row not yet known to be covered
+    for (auto &sp : spans) {
+        for (int r = next; r < sp.first; r++) saved.push_back({r, y[r]});
+        next = std::max(next, sp.second + 1);
+    }
     for (auto &p : pieces) saved.push_back({p.row, y[p.row]});
 
     // Memory pre-check as the reference does (0.8 x free memory, v1.cu:106-116).
@@ -261,51 +267,110 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
 
     bool cuda_ok = true;
     auto ck = [&](cudaError_t e) { cuda_ok = cuda_ok && e == cudaSuccess; };
+    // Large calls run in kChunks nnz-balanced row chunks of the hull: chunk
+    // k's kernels (on a second stream) and its y copy back overlap the
+    // host-to-device copy of chunk k+1's columns and values.  Every row lies
+    // in one chunk.
+    const long long hnnz = rp[hr1 + 1] - rp[hr0];
+    const int kChunks = hnnz >= (8LL << 20) && hm >= 4 * 1024 ? 4 : 1;
+    std::vector<int> cr(kChunks + 1);  // chunk k: hull rows [cr[k], cr[k+1])
+    cr[0] = hr0;
+    cr[kChunks] = hr1 + 1;
+    for (int k = 1; k < kChunks; k++) {
+        const long long target = rp[hr0] + hnnz * k / kChunks;
+        // first row whose nnz start at or after the target
+        int r = (int)(std::lower_bound(rp + cr[k - 1], rp + hr1 + 1, target) - rp);
+        cr[k] = std::min(std::max(r, cr[k - 1]), hr1 + 1);
+    }
+    cudaStream_t s2 = kChunks > 1 ? call_stream(dev, 1) : s;
+    std::vector<cudaEvent_t> ev_copy(kChunks, nullptr);
+    cudaEvent_t ev_done = nullptr;
+    auto destroy_events = [&]() {
+        for (auto &e : ev_copy)
+            if (e) cudaEventDestroy(e);
+        if (ev_done) cudaEventDestroy(ev_done);
+    };
+    for (auto &e : ev_copy) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ck(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    if (!cuda_ok) {
+        destroy_events();
+        cudaEventDestroy(ev);
+        return 1;
+    }
     ck(cudaMemsetAsync(d_st, 0, 4 * sizeof(unsigned), s));
     ck(cudaMemcpyAsync(d_rp64, rp, sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, s));
     launch_rowptr_narrow(d_rp64, d_rp, m, nnz, d_st, s);
     unsigned *h_pin = pinned_words();
-    if (!h_pin) return 1;
+    if (!h_pin) {
+        destroy_events();
+        cudaEventDestroy(ev);
+        return 1;
+    }
     h_pin[0] = 0;
     ck(cudaMemcpyAsync(h_pin, d_st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     ck(cudaEventRecord(ev, s));
     // The big copies queue behind the check and run while the host waits on it.
-    ck(cudaMemcpyAsync(d_col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
-    ck(cudaMemcpyAsync(d_val, val, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
     ck(cudaMemcpyAsync(d_x, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    if (beta != 0.0)
-        ck(cudaMemcpyAsync(d_y, y + hr0, sizeof(double) * hm, cudaMemcpyHostToDevice, s));
+    for (int k = 0; k < kChunks; k++) {
+        const long long lo = k == 0 ? 0 : rp[cr[k]], hi = k + 1 == kChunks ? nnz : rp[cr[k + 1]];
+        ck(cudaMemcpyAsync(d_col + lo, col + lo, sizeof(int) * (hi - lo), cudaMemcpyHostToDevice, s));
+        ck(cudaMemcpyAsync(d_val + lo, val + lo, sizeof(double) * (hi - lo), cudaMemcpyHostToDevice,
+                           s));
+        if (beta != 0.0 && cr[k + 1] > cr[k])
+            ck(cudaMemcpyAsync(d_y + (cr[k] - hr0), y + cr[k], sizeof(double) * (cr[k + 1] - cr[k]),
+                               cudaMemcpyHostToDevice, s));
+        ck(cudaEventRecord(ev_copy[k], s));
+    }
     ck(cudaEventSynchronize(ev));
     cudaEventDestroy(ev);
     const unsigned h_st = h_pin[0];
     if (!cuda_ok || (h_st & ST_BAD_ROWPTR)) {
+        cudaStreamSynchronize(s);
+        destroy_events();
         set_error(cuda_ok ? "row pointer is not monotone within [0, nnz]" : "CUDA copy failed");
         return -1;
     }
 
-    // Natural-extent compute over the hull.
-    Plan p;
-    p.m = hm;
-    p.n = n;
-    p.nnz = (int)(rp[hr1 + 1] - rp[hr0]);
-    p.base = (int)rp[hr0];
-    p.rowptr = d_rp + hr0;
-    p.col = d_col;
-    p.val = d_val;
-    p.status = nullptr;
-    sbb_config cfg{};
-    cfg.kernel = kernel;
-    cfg.persistent = q;
-    int rc = plan_build_unchecked(&p, &cfg, s);
+    // Natural-extent compute, chunk by chunk.
+    std::vector<Plan> plans(kChunks);
+    int rc = SBB_OK;
+    unsigned *pst = h_pin + 1;  // pinned: the status reads stay asynchronous
+    for (int k = 0; k <= kChunks; k++) pst[k] = 0;
+    for (int k = 0; k < kChunks && rc == SBB_OK; k++) {
+        if (cr[k + 1] <= cr[k]) continue;
+        ck(cudaStreamWaitEvent(s2, ev_copy[k], 0));
+        Plan &p = plans[k];
+        p.m = cr[k + 1] - cr[k];
+        p.n = n;
+        p.nnz = (int)(rp[cr[k + 1]] - rp[cr[k]]);
+        p.base = (int)rp[cr[k]];
+        p.rowptr = d_rp + cr[k];
+        p.col = d_col;
+        p.val = d_val;
+        p.status = nullptr;
+        sbb_config cfg{};
+        cfg.kernel = kernel;
+        cfg.persistent = q;
+        rc = plan_build_unchecked(&p, &cfg, s2);
+        if (rc == SBB_OK) rc = plan_run(&p, alpha, d_x, beta, d_y + (cr[k] - hr0), s2);
+        if (rc == SBB_OK && kChunks > 1)  // this chunk's y goes back while the next computes
+            ck(cudaMemcpyAsync(y + cr[k], d_y + (cr[k] - hr0), sizeof(double) * p.m,
+                               cudaMemcpyDeviceToHost, s2));
+        if (rc == SBB_OK && p.status)
+            ck(cudaMemcpyAsync(&pst[k], p.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s2));
+    }
     if (rc != SBB_OK) {
-        plan_free_async(&p, s);
+        cudaStreamSynchronize(s2);
+        cudaStreamSynchronize(s);
+        for (auto &p : plans) plan_free_async(&p, s2);
+        cudaStreamSynchronize(s2);
+        destroy_events();
         return rc == SBB_ERR_NOMEM ? 1 : -1;
     }
-    rc = plan_run(&p, alpha, d_x, beta, d_y, s);
 
-    // Boundary pieces.
+    // Boundary pieces (after every chunk's copy: they read any columns).
     std::vector<double> psum(pieces.size(), 0.0);
-    if (rc == SBB_OK && !pieces.empty()) {
+    if (!pieces.empty()) {
         std::vector<long long> plo(pieces.size()), phi(pieces.size());
         for (size_t i = 0; i < pieces.size(); i++) {
             plo[i] = pieces[i].lo;
@@ -315,7 +380,10 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         long long *d_phi = B.get<long long>(pieces.size());
         double *d_ps = B.get<double>(pieces.size());
         if (!B.ok) {
-            plan_free_async(&p, s);
+            cudaStreamSynchronize(s2);
+            for (auto &p : plans) plan_free_async(&p, s2);
+            cudaStreamSynchronize(s2);
+            destroy_events();
             return 1;
         }
         ck(cudaMemcpyAsync(d_plo, plo.data(), sizeof(long long) * plo.size(),
@@ -326,15 +394,19 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         ck(cudaMemcpyAsync(psum.data(), d_ps, sizeof(double) * psum.size(),
                            cudaMemcpyDeviceToHost, s));
     }
-    unsigned st2[2] = {0, 0};
-    ck(cudaMemcpyAsync(y + hr0, d_y, sizeof(double) * hm, cudaMemcpyDeviceToHost, s));
-    ck(cudaMemcpyAsync(&st2[0], d_st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    if (p.status) ck(cudaMemcpyAsync(&st2[1], p.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    if (kChunks == 1)
+        ck(cudaMemcpyAsync(y + hr0, d_y, sizeof(double) * hm, cudaMemcpyDeviceToHost, s2));
+    ck(cudaMemcpyAsync(pst + kChunks, d_st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    ck(cudaEventRecord(ev_done, s2));
+    ck(cudaStreamWaitEvent(s, ev_done, 0));  // the frees below follow every chunk
     ck(cudaStreamSynchronize(s));
     ck(cudaGetLastError());
-    plan_free_async(&p, s);
-    if (rc != SBB_OK || !cuda_ok) return -1;
-    if (st2[0] | st2[1]) {
+    for (auto &p : plans) plan_free_async(&p, s);
+    destroy_events();
+    if (!cuda_ok) return -1;
+    unsigned st2 = 0;
+    for (int k = 0; k <= kChunks; k++) st2 |= pst[k];
+    if (st2) {
         set_error("column index out of range (or corrupt tile)");
         return -1;
     }
