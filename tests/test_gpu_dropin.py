@@ -137,3 +137,36 @@ def test_dropin_tiny_and_empty(cuda):
     assert api.spMV_mgpu_v1(5, 1, 0, 1.0, np.zeros(1), rp0, np.zeros(1, np.int32), x, 0.5, yy,
                             ngpu=1, kernel=2) == 0
     assert np.array_equal(yy, np.arange(5, dtype=np.float64))
+
+
+@pytest.mark.parametrize("version,kernel", [("baseline", 0), ("v1", 1), ("v1", 2), ("v1", 3),
+                                            ("v2", 2), ("v2", 3)])
+def test_dropin_large_call_chunked(cuda, version, kernel):
+    """Calls with >= 8M nnz copy, compute and copy back in row chunks on two
+    streams; results must match the oracle's drivers like small calls do
+    (empty rows, beta != 0, several v2 tasks)."""
+    from sbb import api, gen
+    A = gen.uniform(41, 450_000, 300_000, 0, 46, p_empty=0.1)
+    m, n, nnz = A.m, A.n, A.nnz
+    assert nnz >= 8 << 20
+    x = gen.uniform_vec(42, n)
+    y = gen.uniform_vec(43, m)
+    alpha, beta = 0.9, -0.7
+    nb = nnz // 3 + 1
+    kk = 1 if kernel == 3 else max(kernel, 1)
+    rc_ref, y_ref = O.dropin(version, m, n, nnz, alpha, A.val, A.rowptr, A.col, x, beta, y,
+                             ngpu=1, kernel=kk, nb=nb, q=2)
+    yy = y.copy()
+    if version == "baseline":
+        rc = api.spMV_mgpu_baseline(m, n, nnz, alpha, A.val, A.rowptr, A.col, x, beta, yy, ngpu=1)
+    elif version == "v1":
+        rc = api.spMV_mgpu_v1(m, n, nnz, alpha, A.val, A.rowptr, A.col, x, beta, yy, ngpu=2,
+                              kernel=kernel)
+    else:
+        rc = api.spMV_mgpu_v2(m, n, nnz, alpha, A.val, A.rowptr, A.col, x, beta, yy, ngpu=2,
+                              kernel=kernel, nb=nb, q=2)
+    assert rc == rc_ref == 0
+    _, sc = O.spmv_dd(A.rowptr, A.col, A.val, x, alpha, beta, y)
+    assert max_scaled_err(yy, y_ref, sc) <= TOL_FP64
+    untouched = y_ref == y
+    assert np.array_equal(yy[untouched], y[untouched])
