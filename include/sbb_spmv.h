@@ -79,7 +79,10 @@ enum {
     SBB_KERNEL_AUTO = 0,
     SBB_KERNEL_VECTOR = 1, /* K1: V lanes per row, warp-shuffle reduce   */
     SBB_KERNEL_MERGE = 2,  /* K2: merge-path split of rows+nnz over CTAs */
-    SBB_KERNEL_TILED = 3   /* K3: CSR5-style 32 x sigma tiles            */
+    SBB_KERNEL_TILED = 3,  /* K3: CSR5-style 32 x sigma tiles            */
+    SBB_KERNEL_LEARNED = 4 /* the trained selector (sbb_mlp_select, built-in
+                              parameters) picks one of the SBB_NUM_CLASSES
+                              batch classes' configurations on the GPU      */
 };
 
 typedef struct {

@@ -38,23 +38,6 @@ struct sbb_batch_s {
     cudaGraphExec_t exec = nullptr;
 };
 
-// The plain-plan configuration of each class.
-static sbb_config class_config(int cls)
-{
-    sbb_config c{};
-    if (cls == kBatchMergeClass) {
-        c.kernel = SBB_KERNEL_MERGE;
-        c.items_per_thread = kBatchIpt;
-    } else if (cls == kBatchTiledClass) {
-        c.kernel = SBB_KERNEL_TILED;
-        c.tile_sigma = kBatchSigma;
-    } else {
-        c.kernel = SBB_KERNEL_VECTOR;
-        c.vector_width = 4 << cls;
-    }
-    return c;
-}
-
 static void batch_free(sbb_batch_s *b)
 {
     if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -172,7 +155,7 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
         p->col = it.col;
         p->val = it.val;
         b->plans.push_back(p);
-        sbb_config c = class_config(it.cls);
+        sbb_config c = batch_class_config(it.cls);
         int rc = plan_build(p, &c, s);
         if (rc != SBB_OK) {
             cudaStreamSynchronize(s);
@@ -407,7 +390,7 @@ int sbb_tune_classes(int m, int n, int nnz, const int *d_rowptr, const int *d_co
         p.rowptr = d_rowptr;
         p.col = d_col;
         p.val = d_val;
-        sbb_config c = class_config(cls);
+        sbb_config c = batch_class_config(cls);
         rc = plan_build(&p, &c, s);
         if (rc == SBB_OK) rc = plan_run(&p, alpha, d_x, beta, d_y, s);  // warm-up
         if (rc == SBB_OK) {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../sbb_internal.h"
@@ -48,6 +49,44 @@ int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *i
     *sigma = 4;
     if (m > 0 && max_row <= 4 * v && max_row <= 128) return SBB_KERNEL_VECTOR;
     return SBB_KERNEL_TILED;
+}
+
+sbb_config batch_class_config(int cls)
+{
+    sbb_config c{};
+    if (cls == kBatchMergeClass) {
+        c.kernel = SBB_KERNEL_MERGE;
+        c.items_per_thread = kBatchIpt;
+    } else if (cls == kBatchTiledClass) {
+        c.kernel = SBB_KERNEL_TILED;
+        c.tile_sigma = kBatchSigma;
+    } else {
+        c.kernel = SBB_KERNEL_VECTOR;
+        c.vector_width = 4 << cls;
+    }
+    return c;
+}
+
+#include "mlp_params.inc"  // kLearnedParams: generated from the trained parameters
+
+// The built-in selector parameters on device `dev` (copied once per device).
+static const float *learned_params(int dev)
+{
+    static std::mutex mu;
+    static float *ptr[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!ptr[dev]) {
+        float *p = nullptr;
+        if (cudaMalloc(&p, sizeof(kLearnedParams)) != cudaSuccess) return nullptr;
+        if (cudaMemcpy(p, kLearnedParams, sizeof(kLearnedParams), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+            cudaFree(p);
+            return nullptr;
+        }
+        ptr[dev] = p;
+    }
+    return ptr[dev];
 }
 
 static int sm_count(int dev)
@@ -128,6 +167,26 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
     }
     sbb_config c{};
     if (cfg) c = *cfg;
+    if (c.kernel == SBB_KERNEL_LEARNED) {
+        // the row pointer was validated above, so the feature pass stays in range
+        if (!validate) {
+            set_error("SBB_KERNEL_LEARNED needs a validated plan");
+            return SBB_ERR_ARG;
+        }
+        const float *params = learned_params(p->device);
+        if (!params) {
+            set_error("selector parameters: device copy failed");
+            return SBB_ERR_CUDA;
+        }
+        int cls = -1;
+        int rc2 = sbb_mlp_select(params, p->m, p->n, p->nnz, p->rowptr, p->col, &cls, s);
+        if (rc2 != SBB_OK) return rc2;
+        if (cls < 0 || cls >= SBB_NUM_CLASSES) {
+            set_error("selector returned no class");
+            return SBB_ERR_CUDA;
+        }
+        c = batch_class_config(cls);
+    }
     int vw = 0, ipt = 0, sigma = 0;
     int k = c.kernel;
     if (k == SBB_KERNEL_AUTO) {

@@ -143,6 +143,8 @@ struct TiledView {
     const CarryRuns *runs;
 };
 bool tiled_view(const Plan *p, TiledView *v);
+// The plain-plan configuration of batch class cls (0 .. SBB_NUM_CLASSES-1).
+sbb_config batch_class_config(int cls);
 // Kernel families of the batch: one persistent kernel each, compiled with
 // only its family's code (so with that code's register budget): vector CSR
 // with 4 or 8 lanes, with 16 or 32 lanes, the merge class, the tiled class.

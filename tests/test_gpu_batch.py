@@ -119,3 +119,47 @@ def test_tuner_times_every_class(cuda):
     d = _mats(1, 7)[0]
     ms = tune(d, reps=3)
     assert len(ms) == NUM_CLASSES and all(t > 0 for t in ms)
+
+
+def test_batch_edge_cases(cuda):
+    """An empty batch; matrices without nnz in every class (y = beta*y, and
+    y = 0 when beta = 0, as a plain launch does); a matrix with no rows."""
+    import torch
+    from sbb.batch import Batch, NUM_CLASSES
+    B = Batch([], [])
+    B.run()
+    B.run_graph()
+    torch.cuda.synchronize()
+    B.check()
+    assert B.launches() == 0
+    B.close()
+    mats, classes = [], []
+    for cls in range(NUM_CLASSES):
+        for beta in (0.0, 0.5):
+            m = 1000 + 37 * cls
+            y = np.random.default_rng(cls).uniform(-1, 1, m)
+            mats.append(dict(m=m, n=50, beta=beta, alpha=2.0, y_h=y,
+                             rowptr=torch.zeros(m + 1, dtype=torch.int32, device="cuda"),
+                             col=torch.zeros(0, dtype=torch.int32, device="cuda"),
+                             val=torch.zeros(0, dtype=torch.float64, device="cuda"),
+                             x=torch.ones(50, dtype=torch.float64, device="cuda"),
+                             y=torch.from_numpy(y).cuda()))
+            classes.append(cls)
+    mats.append(dict(m=0, n=10, rowptr=torch.zeros(1, dtype=torch.int32, device="cuda"),
+                     col=torch.zeros(0, dtype=torch.int32, device="cuda"),
+                     val=torch.zeros(0, dtype=torch.float64, device="cuda"),
+                     x=torch.ones(10, dtype=torch.float64, device="cuda"),
+                     y=torch.zeros(0, dtype=torch.float64, device="cuda"), y_h=np.zeros(0),
+                     beta=0.5))
+    classes.append(5)
+    B = Batch(mats, classes)
+    for run in (B.run, B.run_graph):
+        for d in mats:
+            d["y"].copy_(torch.from_numpy(d["y_h"]))
+        run()
+        torch.cuda.synchronize()
+        B.check()
+        for d, c in zip(mats, classes):
+            want = d["beta"] * d["y_h"] if d["beta"] != 0.0 else np.zeros_like(d["y_h"])
+            assert np.array_equal(d["y"].cpu().numpy(), want), c
+    B.close()

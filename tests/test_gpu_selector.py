@@ -94,3 +94,38 @@ def test_gpu_forward_reproduces_committed_choices(cuda):
     srt = np.sort(y_cpu, axis=1)
     clear = srt[:, 1] - srt[:, 0] > 1e-3
     assert np.array_equal(np.argmin(y_gpu, 1)[clear], np.argmin(y_cpu, 1)[clear])
+
+
+def test_learned_plan_uses_the_selector_and_matches_oracle(cuda):
+    """A SBB_KERNEL_LEARNED plan runs the built-in trained parameters on the
+    GPU: it resolves to the class the selector picks (same configuration as
+    that batch class) and its result matches the oracle."""
+    import torch
+    import oracle as O
+    from helpers import TOL_FP64, max_scaled_err
+    from sbb import gen
+    from sbb.device import Plan
+    sel = S.Selector()  # the committed parameters, the ones built into the library
+    want_cfg = {0: (1, 4), 1: (1, 8), 2: (1, 16), 3: (1, 32), 4: (2, 6), 5: (3, 4)}
+    seen = set()
+    for i in range(9):
+        A = gen.c5(i, 31)
+        d = _dev_csr(A.rowptr32(), A.col, A.m, A.n)
+        cls = sel.select(d)
+        seen.add(cls)
+        x = gen.uniform_vec(7 + i, A.n)
+        y = gen.uniform_vec(8 + i, A.m)
+        P = Plan(d["rowptr"], d["col"], torch.from_numpy(A.val).cuda(), A.n, kernel="learned")
+        info = P.info()
+        k, knob = want_cfg[cls]
+        assert info["kernel"] == k
+        assert knob == {1: info["vector_width"], 2: info["items_per_thread"],
+                        3: info["tile_sigma"]}[k]
+        yy = torch.from_numpy(y).cuda()
+        P.spmv(torch.from_numpy(x).cuda(), yy, 1.0, 0.5)
+        torch.cuda.synchronize()
+        P.check()
+        P.close()
+        ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x, 1.0, 0.5, y)
+        assert max_scaled_err(yy.cpu().numpy(), ref, sc) <= TOL_FP64
+    assert len(seen) >= 2  # the matrices reach more than one class
