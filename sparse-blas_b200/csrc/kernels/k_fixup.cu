@@ -7,10 +7,11 @@
 // tiling, so it is fixed when the plan is built; so are the runs of
 // consecutive tiles carrying the same row (a long row spans many tiles).
 //
-// Run time: one launch.  Blocks [0, short_blocks) take one tile per thread
-// and add single-tile carries; the remaining blocks take one multi-tile run
-// each and add its carries summed in a fixed order (per-thread strided sums,
-// then a shared-memory tree), so results are bit-reproducible.
+// Run time: one launch.  The first blocks take one multi-tile run each and
+// add its carries summed in a fixed order (per-thread strided sums, then a
+// shared-memory tree); the other blocks stride over the tiles and add
+// single-tile carries.  Each row is updated by one thread, so results are
+// bit-reproducible.
 #include "../sbb_internal.h"
 #include "spmv_device.cuh"
 
@@ -57,26 +58,28 @@ __global__ void runs_mark_kernel(const int *__restrict__ crow, int T, int m,
     run_len[j] = lo - t + 1;
 }
 
+// Blocks [0, long_blocks) take the multi-tile runs (launched first: they
+// are the longest); the rest stride over the tiles for single carries.
 __global__ void __launch_bounds__(FT)
 fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cval, int T,
-             const int *__restrict__ run_first, const int *__restrict__ run_len, int short_blocks,
+             const int *__restrict__ run_first, const int *__restrict__ run_len, int long_blocks,
              double alpha, double *__restrict__ y, unsigned *queue, const int *dev_count)
 {
-    if (blockIdx.x < short_blocks) {
-        int t = blockIdx.x * FT + threadIdx.x;
-        if (t == 0 && queue != nullptr) queue[0] = 0u;  // rearm a persistent work queue
-        if (t >= T) return;
-        int r = crow[t];
-        if (r >= m) return;
-        if ((t > 0 && crow[t - 1] == r) || (t + 1 < T && crow[t + 1] == r)) return;
-        fixup_single(y, r, alpha, cval[t]);
+    if (blockIdx.x >= long_blocks) {
+        const int sb = blockIdx.x - long_blocks, nsb = gridDim.x - long_blocks;
+        if (sb == 0 && threadIdx.x == 0 && queue != nullptr) queue[0] = 0u;  // rearm a work queue
+        for (int t = sb * FT + threadIdx.x; t < T; t += nsb * FT) {
+            const int r = crow[t];
+            if (r >= m) continue;
+            if ((t > 0 && crow[t - 1] == r) || (t + 1 < T && crow[t + 1] == r)) continue;
+            fixup_single(y, r, alpha, cval[t]);
+        }
         return;
     }
     __shared__ double s[FT];
     // with a device-side count, a fixed set of blocks strides over the runs
-    const int n_runs = dev_count ? *dev_count : (int)(gridDim.x - short_blocks);
-    const int stride = dev_count ? (int)(gridDim.x - short_blocks) : n_runs;
-    for (int j = blockIdx.x - short_blocks; j < n_runs; j += stride) {
+    const int n_runs = dev_count ? *dev_count : long_blocks;
+    for (int j = blockIdx.x; j < n_runs; j += long_blocks) {
         const int first = run_first[j], len = run_len[j];
         s[threadIdx.x] = fixup_partial(cval, first, len, threadIdx.x);
         __syncthreads();
@@ -139,10 +142,12 @@ void launch_fixup(int m, const int *crow, const double *cval, int T, const Carry
                   double alpha, double *y, unsigned *queue, cudaStream_t s, const int *dev_count)
 {
     if (T <= 0) return;
+    // single carries: one wave of blocks at most, each thread striding over tiles
     int short_blocks = (T + FT - 1) / FT;
-    int long_blocks = dev_count ? 148 : R.n_runs;
+    if (short_blocks > 148 * 8) short_blocks = 148 * 8;
+    const int long_blocks = dev_count ? 148 : R.n_runs;
     fixup_kernel<<<short_blocks + long_blocks, FT, 0, s>>>(m, crow, cval, T, R.run_first,
-                                                           R.run_len, short_blocks, alpha, y,
+                                                           R.run_len, long_blocks, alpha, y,
                                                            queue, dev_count);
 }
 
