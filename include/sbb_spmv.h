@@ -82,7 +82,9 @@ enum {
     SBB_KERNEL_TILED = 3,  /* K3: CSR5-style 32 x sigma tiles            */
     SBB_KERNEL_LEARNED = 4 /* the trained selector (sbb_mlp_select, built-in
                               parameters) picks one of the SBB_NUM_CLASSES
-                              batch classes' configurations on the GPU      */
+                              batch classes' configurations on the GPU; the
+                              parameters (21.6 KB) are copied to a device
+                              the first time it is used and kept until exit */
 };
 
 typedef struct {

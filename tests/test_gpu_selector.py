@@ -75,11 +75,17 @@ def test_select_on_gpu_matches_cpu_argmin(cuda):
     from sbb import gen
     P = S.init_params(np.random.default_rng(4).normal(size=(50, S.N_FEATURES)), 4)
     sel = S.Selector(P)
-    for i in range(6):
+    checked = 0
+    for i in range(8):
         A = gen.c5(i, 77)
         d = _dev_csr(A.rowptr32(), A.col, A.m, A.n)
         y, _ = mlp_cpu.forward(P, mlp_cpu.features(A.rowptr, A.col, A.m, A.n)[None, :])
+        s = np.sort(y[0])
+        if s[1] - s[0] <= 1e-3 * max(1.0, abs(s[0])):
+            continue  # a near-tie: FP32 and FP64 may order it either way
         assert sel.select(d) == int(np.argmin(y[0]))
+        checked += 1
+    assert checked >= 4
 
 
 def test_gpu_forward_reproduces_committed_choices(cuda):
