@@ -6,7 +6,7 @@ compared per row within TOL_FP64 of |alpha|*sum|a_ij x_j| + |beta*y_i|
 (the error metric); return codes and which rows are written must match
 exactly.  The GPU count is pinned to 1, so fixtures made with ngpu > 1 are
 compared with the oracle's ngpu = 1 result.  Kernel 3: the reference's CSR5
-drops alpha and beta; this build honours them, so kernel-3 fixtures are
+drops alpha and beta; this library honours them, so kernel-3 fixtures are
 compared with the reference where alpha = 1, beta = 0 and with the oracle's
 kernel-1 semantics elsewhere.
 """
@@ -43,7 +43,7 @@ def _call(api, c, kernel=None, ngpu=None):
 
 
 def _expected(c):
-    """The reference's result for this call on one GPU with this build's kernel-3 semantics."""
+    """The reference's result for this call on one GPU, with this library's kernel-3 semantics."""
     if c["ngpu"] == 1 and (c["kernel"] != 3 or (c["alpha"] == 1.0 and c["beta"] == 0.0)):
         return c["rc"], c["y_ref"]
     k = 1 if c["kernel"] == 3 else c["kernel"]
