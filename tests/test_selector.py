@@ -77,3 +77,19 @@ def test_committed_data_shapes():
     assert P.shape == (S.N_PARAMS,) and np.all(np.isfinite(P))
     assert E["features"].shape == (512, S.N_FEATURES) and E["times_ms"].shape == (512, 6)
     assert np.all(E["times_ms"] > 0)
+
+
+def test_embedded_parameters_match_the_committed_file(tmp_path):
+    """The build step that puts the trained parameters into libsbb (for
+    SBB_KERNEL_LEARNED plans) writes every float exactly."""
+    import os
+    import re
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    script = os.path.join(here, "..", "sparse-blas_b200", "csrc", "gen", "embed_params.py")
+    out = tmp_path / "p.inc"
+    subprocess.run([sys.executable, script, S.PARAMS_PATH, str(out)], check=True)
+    body = out.read_text().split("{", 1)[1]
+    vals = np.array([float(v) for v in re.findall(r"([-+0-9.e]+)f", body)], np.float32)
+    assert np.array_equal(vals, S.load_params())
