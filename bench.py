@@ -51,6 +51,13 @@ def algo_bytes(m, n, nnz):
 
 def make_workload(name):
     from sbb import gen
+    if name.startswith("mtx:"):  # a Matrix Market file (canonical CSR via the library's reader)
+        from sbb import mmio
+        A = mmio.read(name[4:])
+        x = gen.uniform_vec(51, A.n)
+        y = gen.uniform_vec(52, A.m)
+        return A, x, y, 1.0, 0.5, (f"mtx {A.name}: {A.m} x {A.n}, nnz {A.nnz}, x and y U(-1,1) "
+                                   "seeds 51/52, alpha=1, beta=0.5")
     if name == "c2":
         A = gen.c2()
         x = gen.uniform_vec(21, A.n)
@@ -523,7 +530,7 @@ def run_sbb(args, ws, rank, local):
     peak, peak_kind = peaks()
     achieved = bytes_step / (kern_avg * 1e-3) / 1e9
     tag = {1: "vector_kernel", 2: "merge_kernel", 3: "tiled_kernel"}[info["kernel"]]
-    traffic = traffic_from_profile(tag, args.workload)
+    traffic = traffic_from_profile(tag, args.workload) if not args.workload.startswith("mtx:") else None
 
     # e2e through the reference-facing C ABI with pinned host buffers
     e2e = None
@@ -591,6 +598,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="sbb", choices=["sbb", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--mtx", default=None, help="benchmark a Matrix Market file instead")
     ap.add_argument("--batch-count", type=int, default=512, help="c5: matrices in the batch")
     ap.add_argument("--batch-reps", type=int, default=20, help="c5: timed batch runs")
     ap.add_argument("--kernel", default="tiled", choices=["merge", "vector", "tiled", "auto"])
@@ -605,6 +613,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.mtx:
+        args.workload = "mtx:" + os.path.abspath(args.mtx)
     ws, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

@@ -253,6 +253,22 @@ int sbb_spmv_merge_noalloc(int m, int n, int nnz, const int *d_rowptr,
                            const double *d_x, double beta, double *d_y,
                            void *stream);
 
+/* ---- Matrix Market input ------------------------------------------------- */
+
+/* Loads a Matrix Market coordinate file (fields real / integer / pattern,
+ * symmetry general / symmetric / skew-symmetric) as canonical CSR: rows and
+ * columns sorted, duplicates summed in file order, symmetric storage
+ * expanded, pattern entries set to pattern_value.  Replaces the reader of the
+ * reference's test driver (SparseBLAS/test/dspmv_test.cu:101-136, 228-251),
+ * whose CSR is right only for files already sorted by row.  *handle receives
+ * the matrix (host memory); copy it out with sbb_mm_copy (rowptr: m+1 int64
+ * offsets, col: nnz int32, val: nnz doubles) and release it with
+ * sbb_mm_free.  Errors name the offending line. */
+int sbb_mm_load(const char *path, double pattern_value, void **handle, int *m, int *n,
+                long long *nnz);
+int sbb_mm_copy(void *handle, long long *rowptr, int *col, double *val);
+void sbb_mm_free(void *handle);
+
 const char *sbb_last_error(void);
 
 #ifdef __cplusplus

@@ -91,6 +91,10 @@ SIGNATURES = {
     "sbb_mlp_grad": (C.c_int, [vp, vp, vp, vp, C.c_int, vp, vp, vp]),
     "sbb_mlp_train": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, vp]),
     "sbb_mlp_select": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_int), vp]),
+    "sbb_mm_load": (C.c_int, [C.c_char_p, C.c_double, C.POINTER(vp), C.POINTER(C.c_int),
+                              C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "sbb_mm_copy": (C.c_int, [vp, vp, vp, vp]),
+    "sbb_mm_free": (None, [vp]),
     "sbb_spmv_merge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_double, vp,
                                          C.c_double, vp, vp]),
     "sbb_last_error": (C.c_char_p, []),

@@ -12,6 +12,9 @@ for p in (os.path.join(ROOT, "sparse-blas_b200"), os.path.join(ROOT, "oracle"),
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
+    # temporary files of the tests stay inside the repository (git-ignored)
+    if not config.option.basetemp:
+        config.option.basetemp = os.path.join(ROOT, "tests", ".tmp")
 
 
 @pytest.fixture(scope="session")
