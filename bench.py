@@ -154,14 +154,6 @@ def dist_setup(n_gpus):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        # Each replica sees only its own GPU, as device 0, before any CUDA call:
-        # the host-pointer entry points (GPU count pinned to 1) run on device 0,
-        # like the reference with ngpu = 1, so every rank must own a device 0.
-        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-        ids = [v for v in vis.split(",") if v.strip()] if vis else []
-        os.environ["CUDA_VISIBLE_DEVICES"] = ids[local] if local < len(ids) else str(local)
-        local = 0
     import torch
     if ws > 1:
         import datetime

@@ -24,6 +24,11 @@ extern "C" {
 
 /* ======================= Part 1: drop-in boundary ======================== */
 
+/* The GPU count of these entry points is pinned to 1: a call runs on the
+ * calling thread's current CUDA device (device 0 unless the caller selected
+ * another, as with the reference's ngpu = 1) and returns when y is in host
+ * memory. */
+
 /* Replaces spMV_mgpu_baseline (SparseBLAS/include/spmv_kernel.h:9-13,
  * SparseBLAS/src/dspmv_mgpu_baseline.cu:14-213).  Host pointers; rows split
  * evenly over ngpu parts, which is pinned to 1 here (ngpu <= 0 -> -1). */

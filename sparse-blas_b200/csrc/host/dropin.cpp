@@ -151,16 +151,6 @@ unsigned *pinned_words()
     return w;
 }
 
-struct DeviceGuard {
-    int prev = 0;
-    DeviceGuard(int dev)
-    {
-        cudaGetDevice(&prev);
-        cudaSetDevice(dev);
-    }
-    ~DeviceGuard() { cudaSetDevice(prev); }
-};
-
 struct Buffers {
     cudaStream_t s;
     std::vector<void *> ptrs;
@@ -490,7 +480,8 @@ int dropin_baseline(int m, int n, long long nnz, double *alpha, double *val, lon
 {
     if (ngpu <= 0 || !basic_args_ok(m, n, nnz, alpha, val, rp, col, x, beta, y)) return -1;
     if (m == 0) return 0;
-    DeviceGuard g(0);
+    // one GPU: the calling thread's current device (device 0 unless the
+    // caller selected another), as the reference with ngpu = 1 uses device 0
     auto sl = baseline_slices(m, rp, 1);
     // cusparseDcsrmv picks its own algorithm; the analogue here is the
     // automatic choice (vector CSR for even rows, merge path otherwise).
@@ -506,7 +497,8 @@ int dropin_v1(int m, int n, long long nnz, double *alpha, double *val, long long
     // With nnz == 0 the bisection gives rows [mid, 0]: row 0 alone for m == 1,
     // nothing for m >= 2 (the reference aborts for m >= 4, where dev_m < 0).
     if (m == 0) return 0;
-    DeviceGuard g(0);
+    // one GPU: the calling thread's current device (device 0 unless the
+    // caller selected another), as the reference with ngpu = 1 uses device 0
     auto sl = v1_slices(m, nnz, rp, y, 1);
     return run(m, n, nnz, *alpha, val, rp, col, x, *beta, y, sl, Merge::V1, kernel, 0);
 }
@@ -517,7 +509,8 @@ int dropin_v2(int m, int n, long long nnz, double *alpha, double *val, long long
     if (ngpu <= 0 || q <= 0 || nb <= 0 || kernel < 1 || kernel > 3 ||
         !basic_args_ok(m, n, nnz, alpha, val, rp, col, x, beta, y))
         return -1;
-    DeviceGuard g(0);
+    // one GPU: the calling thread's current device (device 0 unless the
+    // caller selected another), as the reference with ngpu = 1 uses device 0
     // nb clamp of v2.cu:43: 0.8 x free memory / 16 B per nnz / q.
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return -1;

@@ -61,30 +61,3 @@ def test_reference_arm_prints_once_under_torchrun():
     assert d["impl"] == "reference" and d["unit"] == "GB/s" and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
 
-
-def test_each_rank_sees_only_its_own_gpu(monkeypatch):
-    """dist_setup restricts CUDA_VISIBLE_DEVICES to the rank's GPU (so device 0
-    of the single-GPU entry points is the rank's own) before any CUDA call."""
-    sys.path.insert(0, ROOT)
-    import bench
-    calls = {}
-
-    class FakeDist:
-        @staticmethod
-        def init_process_group(backend, timeout=None):
-            calls["backend"] = backend
-
-    import torch
-    monkeypatch.setattr(torch, "distributed", FakeDist, raising=False)
-    monkeypatch.setitem(sys.modules, "torch.distributed", FakeDist)
-    for vis, local, want in ((None, 3, "3"), ("4,5,6,7", 2, "6"), ("", 1, "1")):
-        monkeypatch.setenv("WORLD_SIZE", "4")
-        monkeypatch.setenv("RANK", str(local))
-        monkeypatch.setenv("LOCAL_RANK", str(local))
-        if vis is None:
-            monkeypatch.delenv("CUDA_VISIBLE_DEVICES", raising=False)
-        else:
-            monkeypatch.setenv("CUDA_VISIBLE_DEVICES", vis)
-        ws, rank, loc = bench.dist_setup(4)
-        assert (ws, rank, loc) == (4, local, 0)
-        assert os.environ["CUDA_VISIBLE_DEVICES"] == want
