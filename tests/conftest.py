@@ -14,7 +14,7 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
     # temporary files of the tests stay inside the repository (git-ignored)
     if not config.option.basetemp:
-        config.option.basetemp = os.path.join(ROOT, "tests", ".tmp")
+        config.option.basetemp = os.path.join(ROOT, "tests", "_pytest_tmp")
 
 
 @pytest.fixture(scope="session")
