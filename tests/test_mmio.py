@@ -97,7 +97,7 @@ def test_crlf_comments_blank_lines_and_empty_rows(tmp_path):
 
 
 def test_round_trip_of_a_generated_matrix(tmp_path):
-    A = gen.c5(4)
+    A = gen.uniform(4, 20000, 15000, 0, 12, p_empty=0.05)
     p = tmp_path / "r.mtx"
     mmio.write(p, A)
     B = mmio.read(p)
