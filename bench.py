@@ -16,6 +16,9 @@ metric through the reference-facing C ABI (spMV_mgpu_v1, kernel 2) with host
 buffers in pinned memory: every step copies the matrix, x and y to the GPU and
 y back.  Multi-GPU runs are independent replicas (one per rank, no
 collective); ``value`` sums the ranks' bytes over the slowest rank's time.
+``library_spmv`` (one GPU) times cuSPARSE's SpMV, CSR ALG1 and ALG2, on the
+same resident matrix after the timed region: the vendor library on the same
+GPU, for context (``--no-library`` skips it).
 
 ``--workload c5`` prints the batched form's line instead: 512 seeded
 matrices (banded / power-law / block-diagonal), each matrix's plain launches
@@ -456,6 +459,41 @@ def run_f32(args, ws, rank, local):
     P32.close()
 
 
+def library_spmv(args, m, n, rp, col, val, x, y0, alpha, beta, bytes_step):
+    """cuSPARSE's SpMV (CSR ALG1 and ALG2, the successors of the csrmv and
+    csrmv_mp calls the reference makes) on the same resident matrix, timed
+    with CUDA events on the same stream after the timed region: the vendor
+    library's number on this GPU, for context; none of it is this library's
+    work or counted in `value`."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    try:
+        import cusparse_ref as CS
+        stream = torch.cuda.current_stream()
+        reps = max(3, min(args.steps, 200))
+        out = {"impl": "cusparseSpMV, FP64 values, int32 indices, inputs resident"}
+        for alg in ("alg1", "alg2"):
+            y = y0.clone()
+            op = CS.SpMV(m, n, rp, col, val, x, y, alg, stream)
+            for _ in range(max(args.warmup, 3)):
+                op.run(alpha, beta)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                op.run(alpha, beta)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            op.close()
+            ms = e0.elapsed_time(e1) / reps
+            out[alg] = {"ms_per_call": round(ms, 5),
+                        "GB/s": round(bytes_step / (ms * 1e-3) / 1e9, 2), "calls": reps}
+        return out
+    except Exception as e:  # a comparator only: its absence does not fail the bench
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
 def run_sbb(args, ws, rank, local):
     import ctypes as C
     import torch
@@ -557,6 +595,10 @@ def run_sbb(args, ws, rank, local):
                "sample": f"{reps} full passes of the host CSR loop over this matrix "
                          f"(main.cu:350-356 restated with +beta*y; OpenMP static)"}
 
+    library = None
+    if rank == 0 and ws == 1 and not args.no_library:
+        library = library_spmv(args, m, n, rp, col, val, x, y0, alpha, beta, bytes_step)
+
     if rank == 0:
         line = {
             "metric": "SpMV HBM GB/s (FP64 CSR, algorithmic bytes 12*nnz+4*(m+1)+8*n+16*m)",
@@ -576,6 +618,7 @@ def run_sbb(args, ws, rank, local):
                          "algorithmic_bytes_per_launch": bytes_step},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "library_spmv": library,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
         }
@@ -600,6 +643,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-library", action="store_true",
+                    help="skip the cuSPARSE comparator (library_spmv key)")
     ap.add_argument("--f32", action="store_true",
                     help="time the FP32-storage compensated form against the FP64 plan")
     args = ap.parse_args()
