@@ -123,32 +123,55 @@ struct Piece {
 
 enum class Merge { V1, V2, NONE };
 
+// Per-thread state of the drop-in calls: two streams per device and a few
+// pinned status words, released when the thread ends (so callers that start
+// a thread per call do not accumulate streams or pinned pages).
+struct ThreadState {
+    cudaStream_t s[2][64] = {};
+    bool pool_set[64] = {};
+    unsigned *words = nullptr;
+    ~ThreadState()
+    {
+        for (auto &row : s)
+            for (cudaStream_t st : row)
+                if (st) cudaStreamDestroy(st);
+        if (words) cudaFreeHost(words);
+    }
+};
+ThreadState &thread_state()
+{
+    static thread_local ThreadState t;
+    return t;
+}
+
 // Per-thread stream; device memory comes from the device's default pool,
 // which keeps freed blocks for the next call.
 cudaStream_t call_stream(int dev, int which = 0)
 {
-    static thread_local cudaStream_t s[2][64] = {};
-    static thread_local bool pool_set[64] = {};
+    ThreadState &t = thread_state();
     if (dev < 0 || dev >= 64) return 0;
-    if (!pool_set[dev]) {
+    if (!t.pool_set[dev]) {
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
             unsigned long long keep = ~0ull;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
-        pool_set[dev] = true;
+        t.pool_set[dev] = true;
     }
-    if (!s[which][dev]) cudaStreamCreateWithFlags(&s[which][dev], cudaStreamNonBlocking);
-    return s[which][dev];
+    if (!t.s[which][dev] &&
+        cudaStreamCreateWithFlags(&t.s[which][dev], cudaStreamNonBlocking) != cudaSuccess)
+        t.s[which][dev] = nullptr;
+    return t.s[which][dev];
 }
 
 // A few pinned words per thread, so the status read-back is truly
 // asynchronous and the large copies queued after it overlap the check.
 unsigned *pinned_words()
 {
-    static thread_local unsigned *w = nullptr;
-    if (!w && cudaMallocHost(reinterpret_cast<void **>(&w), 64) != cudaSuccess) w = nullptr;
-    return w;
+    ThreadState &t = thread_state();
+    if (!t.words && cudaMallocHost(reinterpret_cast<void **>(&t.words), 64) != cudaSuccess)
+        t.words = nullptr;
+    return t.words;
 }
 
 struct Buffers {
@@ -243,6 +266,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     int dev = 0;
     cudaGetDevice(&dev);
     cudaStream_t s = call_stream(dev);
+    if (!s) return 1;  // library failure (no stream), as the reference's malloc failures
     Buffers B(s);
     long long *d_rp64 = B.get<long long>((size_t)m + 1);
     int *d_rp = B.get<int>((size_t)m + 1);
@@ -273,6 +297,10 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         cr[k] = std::min(std::max(r, cr[k - 1]), hr1 + 1);
     }
     cudaStream_t s2 = kChunks > 1 ? call_stream(dev, 1) : s;
+    if (!s2) {
+        cudaEventDestroy(ev);
+        return 1;
+    }
     std::vector<cudaEvent_t> ev_copy(kChunks, nullptr);
     cudaEvent_t ev_done = nullptr;
     auto destroy_events = [&]() {

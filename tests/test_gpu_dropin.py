@@ -90,6 +90,81 @@ def test_dropin_random_with_empty_rows(cuda, kernel, version):
         assert max_scaled_err(yy, y_ref, sc) <= TOL_FP64
 
 
+def _dropin_case(seed, version, kernel):
+    """A drop-in call on a seeded matrix with empty and long rows, with the
+    oracle driver's result and the row scale (computed here, on the calling
+    thread)."""
+    m, n = 2000 + 37 * seed, 1800
+    rp, col, val, x, y = rand_csr(500 + seed, m, n, 0, 30, p_empty=0.2,
+                                  long_rows=[(4, 1700), (m - 2, 900)])
+    nnz = int(rp[-1])
+    alpha, beta = 1.0 - 0.1 * seed, (0.0 if seed % 2 else 0.7)
+    nb = max(1, nnz // 5) if version == "v2" else None
+    rc_ref, y_ref = O.dropin(version, m, n, nnz, alpha, val, rp, col, x, beta, y, ngpu=1,
+                             kernel=1 if kernel in (0, 3) else kernel, nb=nb, q=2)
+    assert rc_ref == 0
+    _, sc = O.spmv_dd(rp, col, val, x, alpha, beta, y)
+    return dict(version=version, kernel=kernel, args=(m, n, nnz, alpha, val, rp, col, x, beta),
+                y=y, nb=nb, y_ref=y_ref, sc=sc)
+
+
+def _dropin_call(c):
+    """Runs case c through the drop-in API; returns (rc, max scaled error)."""
+    from sbb import api
+    yy = c["y"].copy()
+    m, n, nnz, alpha, val, rp, col, x, beta = c["args"]
+    if c["version"] == "baseline":
+        rc = api.spMV_mgpu_baseline(m, n, nnz, alpha, val, rp, col, x, beta, yy, ngpu=1)
+    elif c["version"] == "v1":
+        rc = api.spMV_mgpu_v1(m, n, nnz, alpha, val, rp, col, x, beta, yy, ngpu=1,
+                              kernel=c["kernel"])
+    else:
+        rc = api.spMV_mgpu_v2(m, n, nnz, alpha, val, rp, col, x, beta, yy, ngpu=1,
+                              kernel=c["kernel"], nb=c["nb"], q=2)
+    return rc, max_scaled_err(yy, c["y_ref"], c["sc"])
+
+
+CONCURRENT_CALLS = [("baseline", 0), ("v1", 1), ("v1", 2), ("v1", 3), ("v2", 1), ("v2", 2),
+                    ("v2", 3)]
+
+
+def test_dropin_concurrent_callers(cuda):
+    """Drop-in calls from 8 host threads at once (ctypes releases the GIL,
+    so the calls overlap): each thread has its own streams and status words
+    and every result matches the oracle's driver."""
+    from concurrent.futures import ThreadPoolExecutor
+    cases = [_dropin_case(seed, v, k) for seed in range(8) for v, k in CONCURRENT_CALLS]
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        results = list(ex.map(_dropin_call, cases * 2))
+    for c, (rc, err) in zip(cases * 2, results):
+        assert rc == 0 and err <= TOL_FP64, (c["version"], c["kernel"], err)
+
+
+def test_dropin_short_lived_threads(cuda):
+    """Threads that make one call each and end: each ends with its streams
+    and pinned status words released, and 80 of them in turn keep working
+    (no per-thread resources pile up to a failure)."""
+    import threading
+    cases = [_dropin_case(s, v, k) for s in range(2) for v, k in CONCURRENT_CALLS]
+    errors = []
+
+    def one(i):
+        try:
+            rc, err = _dropin_call(cases[i % len(cases)])
+            if rc != 0 or err > TOL_FP64:
+                errors.append((i, rc, err))
+        except Exception as e:  # reported below
+            errors.append((i, repr(e)))
+
+    for wave in range(10):
+        ts = [threading.Thread(target=one, args=(wave * 8 + j,)) for j in range(8)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+    assert not errors, errors
+
+
 def test_dropin_rejects_bad_columns(cuda):
     from sbb import api
     rp, col, val, x, y = rand_csr(1, 50, 40, 1, 5)
