@@ -201,6 +201,14 @@ def cpu_sample_time(A, x, y, alpha, beta, threads, budget_s=12.0):
     return t_total / reps, reps
 
 
+def single_thread(A, x, y, alpha, beta, args):
+    """The same host loop on one thread, as the reference runs it (a few
+    seconds of passes)."""
+    sec, reps = cpu_sample_time(A, x, y, alpha, beta, 1, budget_s=min(args.cpu_budget, 4.0))
+    return {"value": round(algo_bytes(A.m, A.n, A.nnz) / sec / 1e9, 3), "unit": "GB/s",
+            "cores": 1, "sample": f"{reps} full passes"}
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -208,6 +216,7 @@ def run_reference(args, ws, rank):
     threads = os.cpu_count() or 1
     sec, reps = cpu_sample_time(A, x, y, alpha, beta, threads, budget_s=args.cpu_budget)
     gbs = algo_bytes(A.m, A.n, A.nnz) / sec / 1e9
+    one = single_thread(A, x, y, alpha, beta, args)
     line = {
         "metric": "SpMV HBM GB/s (FP64 CSR, algorithmic bytes 12*nnz+4*(m+1)+8*n+16*m)",
         "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
@@ -216,7 +225,8 @@ def run_reference(args, ws, rank):
         "data": "synthetic", "config": {"workload": desc, "nnz": A.nnz, "threads": threads},
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
                          "sample": f"{reps} full passes of the host CSR loop (main.cu:350-356 "
-                                   f"restated with +beta*y, OpenMP static over rows)"},
+                                   f"restated with +beta*y, OpenMP static over rows)",
+                         "single_thread": one},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -593,7 +603,8 @@ def run_sbb(args, ws, rank, local):
         cpu = {"value": round(bytes_step / sec / 1e9, 3), "unit": "GB/s", "cores": threads,
                "kind": "port",
                "sample": f"{reps} full passes of the host CSR loop over this matrix "
-                         f"(main.cu:350-356 restated with +beta*y; OpenMP static)"}
+                         f"(main.cu:350-356 restated with +beta*y; OpenMP static)",
+               "single_thread": single_thread(A, x_h, y_h, alpha, beta, args)}
 
     library = None
     if rank == 0 and ws == 1 and not args.no_library:
