@@ -85,6 +85,26 @@ def test_bad_arguments_rejected_before_any_device_work():
     assert api.spMV_mgpu_baseline(1, 1, 1, 1.0, val, bad_rp, col, x, 0.0, y, ngpu=1) == -1
 
 
+def test_nnz_beyond_int32_rejected_on_the_host():
+    """One GPU takes at most 2^31 - 1 nnz, the reference's own limit (it
+    casts each device's nnz to int, src/dspmv_mgpu_v1.cu:119): larger calls
+    return -1 before any array is read or any device work starts."""
+    from sbb import api
+    rp = np.array([0, 1], np.int64)
+    col = np.zeros(1, np.int32)
+    val = np.ones(1)
+    x = np.ones(1)
+    y = np.zeros(1)
+    for nnz in (2 ** 31, 2 ** 40):
+        assert api.spMV_mgpu_baseline(1, 1, nnz, 1.0, val, rp, col, x, 0.0, y, ngpu=1) == -1
+        for k in (1, 2, 3):
+            assert api.spMV_mgpu_v1(1, 1, nnz, 1.0, val, rp, col, x, 0.0, y, ngpu=1,
+                                    kernel=k) == -1
+            assert api.spMV_mgpu_v2(1, 1, nnz, 1.0, val, rp, col, x, 0.0, y, ngpu=1, kernel=k,
+                                    nb=1 << 20, q=1) == -1
+    assert np.array_equal(y, np.zeros(1))
+
+
 def test_batch_and_tuner_reject_bad_arguments_on_the_host():
     from sbb._lib import lib
     assert lib().sbb_batch_create(None, None, 0, None) == -1
