@@ -151,3 +151,110 @@ def test_full_size_parity(cuda, which):
     for cfg in (dict(kernel="merge", items_per_thread=8), dict(kernel="tiled"), dict(kernel="auto")):
         (out,), _ = run_plan(A.rowptr, A.col, A.val, x, y, A.n, 1.0, beta, cfg)
         assert max_scaled_err(out, y_ref, sc) <= TOL_FP64, cfg
+
+
+
+def _host_bytes_available():
+    """Free host memory for this process: MemAvailable, capped by a cgroup
+    (v2) memory limit when one is set."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    try:
+        with open("/sys/fs/cgroup/memory.max") as f:
+            lim = f.read().strip()
+        if lim != "max":
+            with open("/sys/fs/cgroup/memory.current") as f:
+                cur = int(f.read().strip())
+            room = int(lim) - cur
+            avail = room if avail is None else min(avail, room)
+    except (OSError, ValueError):
+        pass
+    return avail or 0
+
+
+def _wide_matrix():
+    """n = 2^31 - 1 columns, columns 0 and n - 1 in many rows, one row of
+    5,000 nnz across many tiles; integer values and y; alpha = 2, beta = 0.5;
+    with x[c] = c mod 1000 the result (returned as `want`) is exact."""
+    n = 2 ** 31 - 1
+    rng = np.random.default_rng(77)
+    lens = np.full(3000, 9, np.int64)
+    lens[17], lens[2000] = 5000, 700
+    rp = np.zeros(len(lens) + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    nnz = int(rp[-1])
+    col = rng.integers(0, n, nnz).astype(np.int64)
+    col[rp[:-1][::2]] = 0            # first nnz of every other row: column 0
+    col[rp[1:][::3] - 1] = n - 1     # last nnz of every third row: column n - 1
+    val = rng.integers(-5, 6, nnz).astype(np.float64)
+    y0 = 2.0 * rng.integers(-1000, 1000, len(lens)).astype(np.float64)
+    alpha, beta = 2.0, 0.5
+    prod = val * (col % 1000).astype(np.float64)
+    want = alpha * np.add.reduceat(prod, rp[:-1]) + beta * y0  # exact integers
+    return dict(n=n, m=len(lens), nnz=nnz, rp=rp, col=col.astype(np.int32), val=val, y0=y0,
+                alpha=alpha, beta=beta, want=want)
+
+
+def test_column_indices_up_to_int32_max(cuda):
+    """The widest matrix an int32 column index addresses (x is 17 GB on the
+    device): every product and sum is an exact integer in FP64 (and in the
+    FP32-storage form), so each kernel must give the exact result bit for
+    bit whatever its summation order."""
+    import torch
+    from sbb.device import Plan
+    free, _ = torch.cuda.mem_get_info()
+    if free < 40 * 2 ** 30:
+        pytest.skip("needs 40 GiB of free device memory")
+    W = _wide_matrix()
+    n, alpha, beta, want = W["n"], W["alpha"], W["beta"], W["want"]
+    d = torch.device("cuda:0")
+    x = torch.arange(n, dtype=torch.float64, device=d)
+    x.remainder_(1000.0)
+    drp = torch.from_numpy(W["rp"].astype(np.int32)).to(d)
+    dcol = torch.from_numpy(W["col"]).to(d)
+    dval = torch.from_numpy(W["val"]).to(d)
+    dy0 = torch.from_numpy(W["y0"]).to(d)
+    for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="vector", vector_width=32),
+                dict(kernel="merge", items_per_thread=8), dict(kernel="tiled", tile_sigma=4),
+                dict(kernel="tiled", tile_sigma=16), dict(kernel="auto")):
+        P = Plan(drp, dcol, dval, n, **cfg)
+        yy = dy0.clone()
+        P.spmv(x, yy, alpha, beta)
+        torch.cuda.synchronize()
+        P.check()
+        P.close()
+        assert np.array_equal(yy.cpu().numpy(), want), cfg
+    x32 = x.float()
+    P = Plan(drp, dcol, dval.float(), n, kernel="tiled", f32=True)
+    yy = dy0.clone()
+    P.spmv(x32, yy, alpha, beta)
+    torch.cuda.synchronize()
+    P.check()
+    P.close()
+    assert np.array_equal(yy.cpu().numpy(), want), "f32"
+    del x32, x
+    torch.cuda.empty_cache()
+
+
+def test_dropin_column_indices_up_to_int32_max(cuda):
+    """The same matrix through the drop-in, x (17 GB) in host memory."""
+    import torch
+    from sbb import api
+    if _host_bytes_available() < 64 * 2 ** 30:
+        pytest.skip("needs 64 GiB of free host memory")
+    torch.cuda.empty_cache()
+    if torch.cuda.mem_get_info()[0] < 40 * 2 ** 30:
+        pytest.skip("needs 40 GiB of free device memory")
+    W = _wide_matrix()
+    xh = np.arange(W["n"], dtype=np.float64)
+    np.remainder(xh, 1000.0, out=xh)
+    yh = W["y0"].copy()
+    assert api.spMV_mgpu_v1(W["m"], W["n"], W["nnz"], W["alpha"], W["val"], W["rp"], W["col"],
+                            xh, W["beta"], yh, ngpu=1, kernel=3) == 0
+    assert np.array_equal(yh, W["want"])
