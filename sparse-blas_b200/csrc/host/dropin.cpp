@@ -259,7 +259,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return -1;
     const int hm = hr1 - hr0 + 1;
-    double need = (double)nnz * 12.0 + (double)(m + 1) * 12.0 + (double)n * 8.0 + (double)hm * 8.0 +
+    double need = (double)nnz * 12.0 + ((double)m + 1.0) * 12.0 + (double)n * 8.0 + (double)hm * 8.0 +
                   (double)((long long)hm + nnz) / 256.0 * 24.0;
     if (need / 1e9 > 0.8 * ((double)free_b / 1e9)) return -1;
 
@@ -316,7 +316,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         return 1;
     }
     ck(cudaMemsetAsync(d_st, 0, 4 * sizeof(unsigned), s));
-    ck(cudaMemcpyAsync(d_rp64, rp, sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, s));
+    ck(cudaMemcpyAsync(d_rp64, rp, sizeof(long long) * ((size_t)m + 1), cudaMemcpyHostToDevice, s));
     launch_rowptr_narrow(d_rp64, d_rp, m, nnz, d_st, s);
     unsigned *h_pin = pinned_words();
     if (!h_pin) {

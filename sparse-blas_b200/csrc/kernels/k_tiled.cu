@@ -44,6 +44,7 @@ namespace sbb {
 namespace {
 
 constexpr int TW = 4;  // warps per CTA
+constexpr int kTiledMaxRows = 2147483647 - 1024;
 
 struct TiledPlan {
     int sigma = 0, tiles = 0;
@@ -144,7 +145,7 @@ __global__ void tile_seg_kernel(const int *__restrict__ rp, int m, int sigma, in
     long long k = (long long)rp[0] + (long long)t * 32 * sigma;
     int lo = 0, hi = m;  // last r in [0, m) with rp[r] <= k
     while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
+        int mid = lo + ((hi - lo + 1) >> 1);
         if (rp[mid] <= k)
             lo = mid;
         else
@@ -409,6 +410,11 @@ int tiled_sigma(int m, long long nnz, int requested)
 
 int tiled_build(Plan *p, cudaStream_t s)
 {
+    // row counts and segment ranks (plus a tile's few dozen) stay in int
+    if (p->m > kTiledMaxRows) {
+        set_error("tiled plan: at most 2^31 - 1025 rows (use the merge or vector kernel)");
+        return SBB_ERR_ARG;
+    }
     auto *T = new TiledPlan();
     p->tiled = T;
     T->sigma = tiled_sigma(p->m, p->nnz, p->tile_sigma);

@@ -28,7 +28,7 @@ vector_kernel(int m, int n, const int *__restrict__ rowptr, const int *__restric
     constexpr int CR = VectorShape<V>::CR;
     static_assert(CR == vector_chunk_rows(V, V < 4 ? V : 4), "host and device chunk sizes differ");
     const int warps = gridDim.x * (VT / 32);
-    const int chunks = (m + CR - 1) / CR;
+    const int chunks = (int)(((long long)m + CR - 1) / CR);
     const uint64_t stream = l2_evict_first();
     unsigned bad = 0;
     for (int c = blockIdx.x * (VT / 32) + (threadIdx.x >> 5); c < chunks; c += warps)
@@ -46,7 +46,7 @@ void launch_vector_t(const CsrView &A, int V, double alpha, const typename PT::V
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int CR = vector_chunk_rows(V, V < 4 ? V : 4);  // VectorShape<V>::CR
-    long long need = ((long long)(A.m + CR - 1) / CR * 32 + VT - 1) / VT;  // a warp per chunk
+    long long need = (((long long)A.m + CR - 1) / CR * 32 + VT - 1) / VT;  // a warp per chunk
     int grid = (int)(need < (long long)sms * 64 ? need : (long long)sms * 64);
 #define SBB_VL(W)                                                                     \
     case W:                                                                           \

@@ -42,7 +42,7 @@ __device__ __forceinline__ void vector_chunk(int r0, int m, int n, const int *__
     using S = VectorShape<V, UU>;
     constexpr int RPW = S::RPW, U = S::U, CR = S::CR;
     const int lane = threadIdx.x & 31, g = lane / V, li = lane & (V - 1);
-    const bool in = lane < CR && r0 + lane < m;
+    const bool in = lane < CR && lane < m - r0;  // r0 < m: no overflow near INT_MAX
     int rlo = 0, rhi = 0;
     double yv = 0.0;
     if (in) {
@@ -51,15 +51,17 @@ __device__ __forceinline__ void vector_chunk(int r0, int m, int n, const int *__
         if (beta != 0.0) yv = ld_y(y + r0 + lane, stream);
     }
     double out = 0.0;
+    // nnz indices are unsigned: with nnz up to 2^31 - 1 a lane's index runs
+    // to at most nnz - 1 + V (< 2^32), past the int range but never wrapping
 #pragma unroll 1
     for (int j0 = 0; j0 * RPW < CR; j0 += U) {
-        int k[U], hi[U];
+        unsigned k[U], hi[U];
         ACC acc[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int q = (j0 + u) * RPW + g;
-            k[u] = __shfl_sync(0xffffffffu, rlo, q) + li;
-            hi[u] = __shfl_sync(0xffffffffu, rhi, q);
+            k[u] = (unsigned)__shfl_sync(0xffffffffu, rlo, q) + (unsigned)li;
+            hi[u] = (unsigned)__shfl_sync(0xffffffffu, rhi, q);
             acc[u].zero();
         }
         for (;;) {

@@ -258,3 +258,88 @@ def test_dropin_column_indices_up_to_int32_max(cuda):
     assert api.spMV_mgpu_v1(W["m"], W["n"], W["nnz"], W["alpha"], W["val"], W["rp"], W["col"],
                             xh, W["beta"], yh, ngpu=1, kernel=3) == 0
     assert np.array_equal(yh, W["want"])
+
+
+def _max_nnz_matrix(d):
+    """nnz = 2^31 - 1 (the largest an int32 row pointer holds, and the
+    reference's per-device cast): 2^24 rows of 128 nnz, the last of 127, so
+    the last rows end at index 2^31 - 1.  Integer values (+-1..3), x[c] =
+    c mod 1000, integer y, alpha = 2, beta = 0.5: every product and sum is an
+    exact integer, and `want` is the exact result (a row-wise torch
+    reduction in chunks of whole rows)."""
+    import torch
+    nnz, m, L, n = 2 ** 31 - 1, 2 ** 24, 128, 2 ** 20
+    rp = torch.arange(m + 1, dtype=torch.int64, device=d) * L
+    rp[-1] = nnz
+    rp = rp.to(torch.int32)
+    col = torch.empty(nnz, dtype=torch.int32, device=d)
+    val = torch.empty(nnz, dtype=torch.float64, device=d)
+    x = torch.arange(n, dtype=torch.float64, device=d).remainder_(1000.0)
+    rows = torch.empty(m, dtype=torch.float64, device=d)
+    CH = 1 << 27  # whole rows per chunk
+    for s in range(0, nnz, CH):
+        e = min(nnz, s + CH)
+        idx = torch.arange(s, e, dtype=torch.int64, device=d)
+        r, j = idx // L, idx % L
+        c = (r * 37 + j * 5) % n
+        col[s:e] = c.to(torch.int32)
+        v = (1 + j % 3).to(torch.float64) * (1 - 2 * (r % 2)).to(torch.float64)
+        val[s:e] = v
+        p = v * x[c]
+        full = (e - s) // L
+        rows[s // L:s // L + full] = p[:full * L].view(full, L).sum(dim=1)
+        if full * L < e - s:  # the last row (127 nnz)
+            rows[s // L + full] = p[full * L:].sum()
+        del idx, r, j, c, v, p
+    y0 = 2.0 * (torch.arange(m, dtype=torch.float64, device=d).remainder_(2000.0) - 1000.0)
+    alpha, beta = 2.0, 0.5
+    want = (alpha * rows + beta * y0).cpu().numpy()
+    return dict(nnz=nnz, m=m, n=n, rp=rp, col=col, val=val, x=x, y0=y0, alpha=alpha, beta=beta,
+                want=want)
+
+
+def test_nnz_at_int32_max(cuda):
+    """Every kernel on a matrix of 2^31 - 1 nnz, bit for bit (the vector
+    kernel's lanes step past index 2^31 - 1 on the last rows)."""
+    import torch
+    from sbb.device import Plan
+    torch.cuda.empty_cache()
+    if torch.cuda.mem_get_info()[0] < 100 * 2 ** 30:
+        pytest.skip("needs 100 GiB of free device memory")
+    W = _max_nnz_matrix(cuda)
+    for cfg in (dict(kernel="vector", vector_width=32), dict(kernel="vector", vector_width=4),
+                dict(kernel="merge", items_per_thread=8), dict(kernel="tiled", tile_sigma=4),
+                dict(kernel="auto")):
+        P = Plan(W["rp"], W["col"], W["val"], W["n"], **cfg)
+        yy = W["y0"].clone()
+        P.spmv(W["x"], yy, W["alpha"], W["beta"])
+        torch.cuda.synchronize()
+        P.check()
+        P.close()
+        assert np.array_equal(yy.cpu().numpy(), W["want"]), cfg
+    del W
+    torch.cuda.empty_cache()
+
+
+def test_dropin_nnz_at_int32_max(cuda):
+    """The same matrix through spMV_mgpu_v1 (kernels 1 and 3) from host
+    memory (26 GB of columns and values)."""
+    import torch
+    from sbb import api
+    if _host_bytes_available() < 96 * 2 ** 30:
+        pytest.skip("needs 96 GiB of free host memory")
+    torch.cuda.empty_cache()
+    if torch.cuda.mem_get_info()[0] < 100 * 2 ** 30:
+        pytest.skip("needs 100 GiB of free device memory")
+    W = _max_nnz_matrix(cuda)
+    rp = W["rp"].cpu().numpy().astype(np.int64)
+    rp[-1] = W["nnz"]
+    col, val, x, y0 = (W[k].cpu().numpy() for k in ("col", "val", "x", "y0"))
+    want, alpha, beta, m, n, nnz = (W[k] for k in ("want", "alpha", "beta", "m", "n", "nnz"))
+    del W
+    torch.cuda.empty_cache()
+    for kernel in (1, 3):
+        yh = y0.copy()
+        assert api.spMV_mgpu_v1(m, n, nnz, alpha, val, rp, col, x, beta, yh, ngpu=1,
+                                kernel=kernel) == 0
+        assert np.array_equal(yh, want), kernel
