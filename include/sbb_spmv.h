@@ -27,7 +27,9 @@ extern "C" {
 /* The GPU count of these entry points is pinned to 1: a call runs on the
  * calling thread's current CUDA device (device 0 unless the caller selected
  * another, as with the reference's ngpu = 1) and returns when y is in host
- * memory. */
+ * memory.  nnz <= 2^31 - 1 (the reference casts a device's nnz to int,
+ * SparseBLAS/src/dspmv_mgpu_v1.cu:119; larger calls return -1); kernel 3
+ * takes at most 2^31 - 1025 rows. */
 
 /* Replaces spMV_mgpu_baseline (SparseBLAS/include/spmv_kernel.h:9-13,
  * SparseBLAS/src/dspmv_mgpu_baseline.cu:14-213).  Host pointers; rows split
