@@ -48,7 +48,7 @@ int default_kernel_choice(int m, int nnz, int max_row, int *vector_width, int *i
     *ipt = 6;
     *sigma = 4;
     if (m > 0 && max_row <= 4 * v && max_row <= 128) return SBB_KERNEL_VECTOR;
-    return SBB_KERNEL_TILED;
+    return m > kTiledMaxRows ? SBB_KERNEL_MERGE : SBB_KERNEL_TILED;
 }
 
 sbb_config batch_class_config(int cls)
@@ -186,6 +186,8 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
             return SBB_ERR_CUDA;
         }
         c = batch_class_config(cls);
+        if (c.kernel == SBB_KERNEL_TILED && p->m > kTiledMaxRows)
+            c = batch_class_config(kBatchMergeClass);
     }
     int vw = 0, ipt = 0, sigma = 0;
     int k = c.kernel;

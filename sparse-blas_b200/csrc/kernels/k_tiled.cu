@@ -44,7 +44,6 @@ namespace sbb {
 namespace {
 
 constexpr int TW = 4;  // warps per CTA
-constexpr int kTiledMaxRows = 2147483647 - 1024;
 
 struct TiledPlan {
     int sigma = 0, tiles = 0;

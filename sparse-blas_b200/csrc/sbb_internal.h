@@ -32,6 +32,10 @@ enum : unsigned {
 
 // ---- kernel launchers (defined in the .cu files) ---------------------------
 constexpr int kMergeThreads = 256;
+// Tile plans take at most this many rows: row counts and segment ranks plus
+// a tile's offsets stay in int.  The automatic and learned choices use the
+// merge path above it.
+constexpr int kTiledMaxRows = 2147483647 - 1024;
 
 struct CsrView {          // rows [0, m) of a CSR matrix; offsets are absolute
     int m, n;

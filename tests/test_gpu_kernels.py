@@ -343,3 +343,53 @@ def test_dropin_nnz_at_int32_max(cuda):
         assert api.spMV_mgpu_v1(m, n, nnz, alpha, val, rp, col, x, beta, yh, ngpu=1,
                                 kernel=kernel) == 0
         assert np.array_equal(yh, want), kernel
+
+
+def test_rows_at_int32_max(cuda):
+    """m = 2^31 - 1 rows (row pointer 8.6 GB, y 17 GB): one nnz in every
+    128th row and 10,000 in row 5.  The vector and merge kernels and the
+    automatic choice (the merge path here: a long row, and more rows than a
+    tile plan takes) give the exact result bit for bit; an explicit tile
+    plan is refused with an error, not run."""
+    import torch
+    from sbb.device import Plan, SbbError
+    torch.cuda.empty_cache()
+    if torch.cuda.mem_get_info()[0] < 100 * 2 ** 30:
+        pytest.skip("needs 100 GiB of free device memory")
+    d = cuda
+    m, n, long_row, long_len = 2 ** 31 - 1, 2 ** 20, 5, 10000
+    # rowptr[r] = ceil(r / 128) + long_len * (r > long_row), in chunks
+    rp = torch.empty(m + 1, dtype=torch.int32, device=d)
+    CH = 1 << 28
+    for s in range(0, m + 1, CH):
+        r = torch.arange(s, min(m + 1, s + CH), dtype=torch.int64, device=d)
+        rp[s:s + len(r)] = ((r + 127) // 128 + long_len * (r > long_row)).to(torch.int32)
+        del r
+    nnz = int(rp[-1].item())
+    k = torch.arange(nnz, dtype=torch.int64, device=d)
+    col = ((k * 37) % n).to(torch.int32)
+    val = ((1 + k % 3) * (1 - 2 * (k % 2))).to(torch.float64)
+    x = torch.arange(n, dtype=torch.float64, device=d).remainder_(1000.0)
+    # row of nnz k: 0 for k = 0, the long row for k <= long_len, then every
+    # 128th row in turn
+    row_of = torch.where(k == 0, 0, torch.where(k <= long_len, long_row, (k - long_len) * 128))
+    want = torch.zeros(m, dtype=torch.float64, device=d)
+    want.index_add_(0, row_of, val * x[col.long()])  # exact integers
+    del k, row_of
+    y0 = torch.arange(m, dtype=torch.float64, device=d).remainder_(2000.0).sub_(1000.0).mul_(2.0)
+    alpha, beta = 2.0, 0.5
+    want.mul_(alpha).add_(y0, alpha=beta)
+    yy = torch.empty_like(y0)
+    for cfg in (dict(kernel="vector", vector_width=4), dict(kernel="merge", items_per_thread=8),
+                dict(kernel="auto")):
+        P = Plan(rp, col, val, n, **cfg)
+        if cfg["kernel"] == "auto":
+            assert P.info()["kernel"] == 2  # the merge path
+        yy.copy_(y0)
+        P.spmv(x, yy, alpha, beta)
+        torch.cuda.synchronize()
+        P.check()
+        P.close()
+        assert torch.equal(yy, want), cfg
+    with pytest.raises(SbbError):
+        Plan(rp, col, val, n, kernel="tiled")
