@@ -131,7 +131,8 @@ int sbb_plan_create_f32(sbb_plan_t *plan, int m, int n, int nnz,
                         const float *d_val, const sbb_config *cfg, void *stream);
 /* y = alpha*A*x + beta*y on the stream (asynchronous).  y is not read when
  * beta == 0.  Out-of-range column indices are skipped and flagged; see
- * sbb_plan_check. */
+ * sbb_plan_check.  x (n values) and y (m values) must not overlap
+ * (SBB_ERR_ARG): the kernels read x while they write y. */
 int sbb_spmv(sbb_plan_t plan, double alpha, const double *d_x, double beta,
              double *d_y, void *stream);
 int sbb_spmv_f32(sbb_plan_t plan, double alpha, const float *d_x, double beta,
@@ -187,7 +188,8 @@ int sbb_batch_create(sbb_batch_t *batch, const sbb_batch_item *items, int count,
  * and joined back, then one more launch adds the carries of every merge/tiled
  * matrix and finishes the empty rows of tiled ones.  Each matrix's y is
  * bit-identical to sbb_batch_run_each with the same classes.  The y arrays
- * must not overlap. */
+ * must not overlap one another or any x (sbb_batch_create checks; x arrays
+ * may be shared). */
 int sbb_batch_run(sbb_batch_t batch, void *stream);
 /* Same launches, captured once in a CUDA graph and replayed. */
 int sbb_batch_run_graph(sbb_batch_t batch, void *stream);
@@ -248,7 +250,8 @@ int sbb_mlp_select(const float *d_params, int m, int n, int nnz, const int *d_ro
  * that may not block on the allocator, a host framework that owns all device
  * memory), the scratch lives in a fixed 5 MiB __device__ array of the library,
  * held on every GPU that loads it until the process exits.  Limit:
- * m + nnz <= 100,663,296 (larger inputs return SBB_ERR_ARG).  All calls share
+ * m + nnz <= 100,663,296 (larger inputs return SBB_ERR_ARG); x and y must
+ * not overlap (SBB_ERR_ARG).  All calls share
  * that array and it keeps the last call's contents, so calls that overlap on
  * the GPU race; serialise them.  The first call on a device looks up the
  * array's address; make it before any stream capture on that device.  The row

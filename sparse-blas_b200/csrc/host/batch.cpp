@@ -98,6 +98,40 @@ static int enqueue(sbb_batch_s *b, cudaStream_t s)
 
 extern "C" {
 
+// The y arrays must not overlap one another or any item's x (a matrix's
+// kernels write its y while the others read their x); x arrays may be
+// shared.  Sorted y ranges, then one search per x: O(count log count).
+static bool batch_ranges_ok(const sbb_batch_item *items, int count)
+{
+    std::vector<std::pair<uintptr_t, uintptr_t>> ys;  // [start, end) of each y
+    for (int i = 0; i < count; i++)
+        if (items[i].y && items[i].m > 0) {
+            const auto a = reinterpret_cast<uintptr_t>(items[i].y);
+            ys.push_back({a, a + 8 * (size_t)items[i].m});
+        }
+    std::sort(ys.begin(), ys.end());
+    for (size_t j = 1; j < ys.size(); j++)
+        if (ys[j].first < ys[j - 1].second) {
+            set_error("batch: two items' y arrays overlap");
+            return false;
+        }
+    // the y ranges are now disjoint and sorted, so their ends are sorted too
+    for (int i = 0; i < count; i++) {
+        if (!items[i].x || items[i].n <= 0) continue;
+        const auto a = reinterpret_cast<uintptr_t>(items[i].x);
+        const uintptr_t e = a + 8 * (size_t)items[i].n;
+        auto k = std::lower_bound(ys.begin(), ys.end(), a,
+                                  [](const std::pair<uintptr_t, uintptr_t> &iv, uintptr_t v) {
+                                      return iv.second <= v;
+                                  });
+        if (k != ys.end() && k->first < e) {
+            set_error("batch: item " + std::to_string(i) + "'s x overlaps a y array");
+            return false;
+        }
+    }
+    return true;
+}
+
 int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, void *stream)
 {
     if (!out || count < 0 || (count > 0 && !items)) {
@@ -105,6 +139,7 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
         return SBB_ERR_ARG;
     }
     *out = nullptr;
+    if (!batch_ranges_ok(items, count)) return SBB_ERR_ARG;
     auto s = static_cast<cudaStream_t>(stream);
     auto *b = new sbb_batch_s();
     cudaGetDevice(&b->device);

@@ -362,6 +362,15 @@ int sbb_plan_create_f32(sbb_plan_t *plan, int m, int n, int nnz, const int *d_ro
     return create_common(plan, m, n, nnz, d_rowptr, d_col, d_val, true, cfg, stream);
 }
 
+// x (n values) overlapping y (m doubles): an error, set here.
+static bool xy_overlap(const sbb_plan_s *plan, const void *d_x, const double *d_y)
+{
+    const size_t xb = (size_t)plan->p.n * (plan->p.f32 ? 4 : 8), yb = (size_t)plan->p.m * 8;
+    if (!ranges_overlap(d_x, xb, d_y, yb)) return false;
+    set_error("x and y overlap (the kernels read x while they write y)");
+    return true;
+}
+
 int sbb_spmv(sbb_plan_t plan, double alpha, const double *d_x, double beta, double *d_y,
              void *stream)
 {
@@ -369,6 +378,7 @@ int sbb_spmv(sbb_plan_t plan, double alpha, const double *d_x, double beta, doub
         set_error("bad sbb_spmv arguments (NULL pointer or an FP32 plan)");
         return SBB_ERR_ARG;
     }
+    if (xy_overlap(plan, d_x, d_y)) return SBB_ERR_ARG;
     return plan_run(&plan->p, alpha, d_x, beta, d_y, static_cast<cudaStream_t>(stream));
 }
 
@@ -379,6 +389,7 @@ int sbb_spmv_f32(sbb_plan_t plan, double alpha, const float *d_x, double beta, d
         set_error("bad sbb_spmv_f32 arguments (NULL pointer or an FP64 plan)");
         return SBB_ERR_ARG;
     }
+    if (xy_overlap(plan, d_x, d_y)) return SBB_ERR_ARG;
     return plan_run(&plan->p, alpha, d_x, beta, d_y, static_cast<cudaStream_t>(stream));
 }
 
@@ -389,6 +400,7 @@ int sbb_spmv_timed(sbb_plan_t plan, double alpha, const void *d_x, double beta, 
         set_error("bad sbb_spmv_timed arguments");
         return SBB_ERR_ARG;
     }
+    if (xy_overlap(plan, d_x, d_y)) return SBB_ERR_ARG;
     TimingHooks &h = timing_hooks();
     h.start = static_cast<cudaEvent_t>(ev_start);
     h.stop = static_cast<cudaEvent_t>(ev_stop);

@@ -91,6 +91,10 @@ extern "C" int sbb_spmv_merge_noalloc(int m, int n, int nnz, const int *d_rowptr
                   std::to_string(kMaxSegments * kItems) + " merge items");
         return SBB_ERR_ARG;
     }
+    if (ranges_overlap(d_x, (size_t)n * 8, d_y, (size_t)m * 8)) {
+        set_error("sbb_spmv_merge_noalloc: x and y overlap");
+        return SBB_ERR_ARG;
+    }
     if (m == 0) return SBB_OK;
     int dev = 0;
     SBB_CUDA(cudaGetDevice(&dev));

@@ -21,6 +21,16 @@ void set_error(const std::string &msg);
         }                                                                     \
     } while (0)
 
+// True when the byte ranges [a, a + abytes) and [b, b + bbytes) share a byte.
+// x must not overlap y: the kernels read x while they write y (cuSPARSE's
+// SpMV has the same rule).
+inline bool ranges_overlap(const void *a, size_t abytes, const void *b, size_t bbytes)
+{
+    if (!a || !b || abytes == 0 || bbytes == 0) return false;
+    const uintptr_t pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    return pa < pb + bbytes && pb < pa + abytes;
+}
+
 // Device status word bits, written by kernels instead of trapping.
 enum : unsigned {
     ST_BAD_ROWPTR = 1u << 0,   // non-monotone row pointer or out of [0, nnz]

@@ -105,6 +105,40 @@ def test_nnz_beyond_int32_rejected_on_the_host():
     assert np.array_equal(y, np.zeros(1))
 
 
+def test_overlapping_x_and_y_rejected_on_the_host():
+    """x must not overlap y (the kernels read x while they write y): the
+    no-allocation entry point and batch creation refuse such calls before any
+    device work (the pointers here are never dereferenced)."""
+    import ctypes as C
+    from sbb._lib import BatchItem, last_error, lib
+    base = 1 << 32
+    p = lambda off: C.c_void_p(base + off)  # noqa: E731
+    m, n = 100, 100
+    # y starts inside x
+    rc = lib().sbb_spmv_merge_noalloc(m, n, 10, p(0), p(1 << 20), p(2 << 20), 1.0, p(0), 0.0,
+                                      p(8 * 50), None)
+    assert rc == -1 and "overlap" in last_error()
+
+    def items(*specs):
+        arr = (BatchItem * len(specs))()
+        for it, (xo, yo) in zip(arr, specs):
+            it.m, it.n, it.nnz = m, n, 10
+            it.rowptr, it.col, it.val = base + (3 << 20), base + (4 << 20), base + (5 << 20)
+            it.x, it.y = base + xo, base + yo
+            it.alpha, it.beta, it.cls = 1.0, 0.0, 0
+        return arr
+
+    h = C.c_void_p()
+    # two y arrays overlapping
+    arr = items((0, 8 << 20), (1 << 16, (8 << 20) + 8 * 99))
+    assert lib().sbb_batch_create(C.byref(h), arr, 2, None) == -1
+    assert "y arrays overlap" in last_error()
+    # item 1's x overlapping item 0's y (a shared x is allowed)
+    arr = items((0, 8 << 20), ((8 << 20) + 8 * 10, 9 << 20), (0, 10 << 20))
+    assert lib().sbb_batch_create(C.byref(h), arr, 3, None) == -1
+    assert "item 1's x overlaps" in last_error()
+
+
 def test_batch_and_tuner_reject_bad_arguments_on_the_host():
     from sbb._lib import lib
     assert lib().sbb_batch_create(None, None, 0, None) == -1

@@ -116,6 +116,25 @@ def test_bad_column_rejected_by_tiled_plan(cuda):
         Plan(drp, dcol, dval, len(x), kernel="tiled")
 
 
+
+def test_overlapping_x_and_y_rejected(cuda):
+    """x must not overlap y (the kernels read x while they write y): refused
+    with an error; adjacent, non-overlapping views of one buffer are fine."""
+    import torch
+    from sbb.device import Plan, SbbError
+    rp, col, val, x, y = MATS["uniform"]()  # 5000 x 4000
+    drp, dcol, dval, _, _ = to_dev(rp, col, val, x, y)
+    buf = torch.zeros(9000, dtype=torch.float64, device="cuda")
+    for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="merge"), dict(kernel="tiled")):
+        P = Plan(drp, dcol, dval, 4000, **cfg)
+        with pytest.raises(SbbError):
+            P.spmv(buf[:4000], buf[3999:8999], 1.0, 0.0)
+        P.spmv(buf[:4000], buf[4000:9000], 1.0, 0.0)
+        torch.cuda.synchronize()
+        P.check()
+        P.close()
+    assert torch.count_nonzero(buf) == 0
+
 def test_bad_rowptr_rejected_at_plan(cuda):
     from sbb.device import Plan, SbbError
     rp, col, val, x, y = MATS["uniform"]()
