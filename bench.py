@@ -626,6 +626,7 @@ def run_sbb(args, ws, rank, local):
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "peak_source": peak_kind,
                          "kernel_ms_avg": round(kern_avg, 5),
+                         "kernel_ms_median": round(statistics.median(kern_ms), 5),
                          "algorithmic_bytes_per_launch": bytes_step},
             "cpu_baseline": cpu,
             "e2e": e2e,
