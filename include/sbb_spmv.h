@@ -281,6 +281,31 @@ void sbb_mm_free(void *handle);
 
 const char *sbb_last_error(void);
 
+/* ---- test hooks ------------------------------------------------------------ */
+
+/* Host-side fault injection for the library's own tests, so that the error
+ * paths of the reference's contract run without faulting a GPU: the 1 a
+ * drop-in call returns when a device allocation fails
+ * (SparseBLAS/src/dspmv_mgpu_baseline.cu:99-135), the -1 of the 0.8 x
+ * free-memory pre-check (SparseBLAS/src/dspmv_mgpu_v1.cu:104-116), and the
+ * timeout status of the tiled kernel's bounded waits.  Process-wide; not for
+ * production use.
+ *   SBB_TEST_RESET        disarm every hook (value ignored);
+ *   SBB_TEST_FAIL_ALLOC   value = k >= 1: the k-th device allocation the
+ *                         library makes from now on fails, once (0 disarms);
+ *   SBB_TEST_FREE_BYTES   value >= 0: the drop-in memory pre-check sees at
+ *                         most this many free bytes (< 0 disarms);
+ *   SBB_TEST_WAIT_BUDGET  value >= 0: in tiled-kernel launches the first wait
+ *                         of the grid's first warp for its tile copy gives up
+ *                         after `value` polls (0: at once); the kernel then
+ *                         lets its copies in flight land, raises the timeout
+ *                         status and stops, so sbb_plan_check reports
+ *                         SBB_ERR_INPUT and drop-in calls return -1 (< 0
+ *                         disarms). */
+enum { SBB_TEST_RESET = 0, SBB_TEST_FAIL_ALLOC = 1, SBB_TEST_FREE_BYTES = 2,
+       SBB_TEST_WAIT_BUDGET = 3 };
+int sbb_test_hook(int what, long long value);
+
 #ifdef __cplusplus
 }
 #endif

@@ -183,7 +183,7 @@ struct Buffers {
     T *get(size_t count)
     {
         void *p = nullptr;
-        if (cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s) != cudaSuccess) {
+        if (dev_malloc_async(&p, std::max<size_t>(count, 1) * sizeof(T), s) != cudaSuccess) {
             ok = false;
             return nullptr;
         }
@@ -258,6 +258,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     // Memory pre-check as the reference does (0.8 x free memory, v1.cu:106-116).
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return -1;
+    free_b = capped_free_bytes(free_b);
     const int hm = hr1 - hr0 + 1;
     double need = (double)nnz * 12.0 + ((double)m + 1.0) * 12.0 + (double)n * 8.0 + (double)hm * 8.0 +
                   (double)((long long)hm + nnz) / 256.0 * 24.0;
@@ -422,16 +423,17 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     for (auto &p : plans) plan_free_async(&p, s);
     destroy_events();
     if (!cuda_ok) return -1;
+    // Restore the rows the reference never writes, and the special rows'
+    // inputs for the merge.  This comes before the status check, so a call
+    // that fails on bad column indices still leaves every row outside the
+    // slices with its input value (the covered rows then hold partial sums).
+    for (auto &sv : saved) y[sv.first] = sv.second;
     unsigned st2 = 0;
     for (int k = 0; k <= kChunks; k++) st2 |= pst[k];
     if (st2) {
         set_error("column index out of range (or corrupt tile)");
         return -1;
     }
-
-    // Restore the rows the reference never writes, and the special rows'
-    // inputs for the merge.
-    for (auto &sv : saved) y[sv.first] = sv.second;
     std::vector<double> y0(pieces.size());
     for (size_t i = 0; i < pieces.size(); i++) y0[i] = y[pieces[i].row];
 
@@ -542,6 +544,7 @@ int dropin_v2(int m, int n, long long nnz, double *alpha, double *val, long long
     // nb clamp of v2.cu:43: 0.8 x free memory / 16 B per nnz / q.
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return -1;
+    free_b = capped_free_bytes(free_b);
     long long cap = (long long)(0.8 * ((double)free_b / 1e9) * 1e9 / 16.0) / q;
     nb = std::min(nb, cap);
     if (nb <= 0) return -1;

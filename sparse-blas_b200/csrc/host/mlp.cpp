@@ -19,7 +19,7 @@ struct Scratch {
     explicit Scratch(cudaStream_t st) : s(st) {}
     bool get(size_t bytes)
     {
-        if (cudaMallocAsync(&p, bytes ? bytes : 16, s) != cudaSuccess) {
+        if (dev_malloc_async(&p, bytes ? bytes : 16, s) != cudaSuccess) {
             set_error("selector: device allocation failed");
             p = nullptr;
             return false;

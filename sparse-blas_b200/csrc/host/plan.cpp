@@ -100,7 +100,7 @@ template <typename T>
 static int dalloc(T **p, size_t count, cudaStream_t s, size_t *acc)
 {
     size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(p), bytes, s);
+    cudaError_t e = dev_malloc_async(reinterpret_cast<void **>(p), bytes, s);
     if (e != cudaSuccess) {
         *p = nullptr;
         set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));

@@ -196,12 +196,15 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
                         ? (__ldg(reinterpret_cast<const unsigned *>(
                                M.blob + (size_t)(t0 + nt) * TBB + kBit0)) & 1u)
                         : 0u;
-                const bool ok = mbar_wait(bar0 + 8 * cur, (phases >> cur) & 1u);
-                phases ^= 1u << cur;
-                if (!ok) {
+                if (!mbar_wait(bar0 + 8 * cur, (phases >> cur) & 1u)) {
+                    // let the copies still in flight land (bounded) before the
+                    // warp leaves: this unit's and, if started, the next one's
+                    mbar_wait(bar0 + 8 * cur, (phases >> cur) & 1u);
+                    if (pre_k >= 0) mbar_wait(bar0 + 8 * pre_s, (phases >> pre_s) & 1u);
                     timeout = 1;
                     break;
                 }
+                phases ^= 1u << cur;  // flips only once the copy has landed
                 const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
                 const unsigned char *tb = warp_smem<FAM>() + cur * TG * TBB;
                 double xv[kBatchSigma], xn[kBatchSigma];
@@ -229,11 +232,7 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
         }
     }
     if constexpr (kTiled) {
-        if (timeout) {
-            // let a copy still in flight land (bounded) before the warp leaves
-            if (pre_k >= 0) mbar_wait(bar0 + 8 * pre_s, (phases >> pre_s) & 1u);
-            if (lane == 0) atomicOr(status, ST_TIMEOUT);
-        }
+        if (timeout && lane == 0) atomicOr(status, ST_TIMEOUT);
     }
     if (bad) atomicOr(status, ST_BAD_COL);
 }

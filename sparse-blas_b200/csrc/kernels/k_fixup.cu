@@ -101,9 +101,9 @@ int carry_runs_build(const int *crow, int T, int m, CarryRuns *R, cudaStream_t s
     if (T <= 0) return SBB_OK;
     int cap = T / 2 + 1;
     int *count = nullptr;
-    if (cudaMallocAsync((void **)&R->run_first, sizeof(int) * cap, s) != cudaSuccess ||
-        cudaMallocAsync((void **)&R->run_len, sizeof(int) * cap, s) != cudaSuccess ||
-        cudaMallocAsync((void **)&count, sizeof(int), s) != cudaSuccess) {
+    if (dev_malloc_async((void **)&R->run_first, sizeof(int) * cap, s) != cudaSuccess ||
+        dev_malloc_async((void **)&R->run_len, sizeof(int) * cap, s) != cudaSuccess ||
+        dev_malloc_async((void **)&count, sizeof(int), s) != cudaSuccess) {
         set_error("carry runs: device allocation failed");
         return SBB_ERR_NOMEM;
     }

@@ -21,7 +21,11 @@
 //     give wrong results - serialise them;
 //   * the first call on a device looks up the array's device address (an
 //     ordinary host-side step); make that first call before any stream
-//     capture on that device.
+//     capture on that device.  The address is kept per device together with
+//     the identity of the context it was found in, and looked up again when
+//     that context has been replaced (after cudaDeviceReset, for example).
+#include <cuda.h>  // driver types only; the entry points are fetched at run time
+
 #include <mutex>
 
 #include "../sbb_internal.h"
@@ -46,24 +50,61 @@ constexpr size_t kScratchBytes = 2 * kCoordBytes + kCarryBytes + 2 * kRunBytes +
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_mu;
-void *g_scratch_addr[64] = {};
+struct ScratchAddr {
+    void *ptr = nullptr;
+    unsigned long long ctx = 0;  // identity of the context the address belongs to
+};
+ScratchAddr g_scratch_addr[64];
 
-// Device address of the scratch on device `dev` (looked up once per device,
-// with that device current).
+// Unique id of the calling thread's current context, or 0 when there is none
+// or the driver cannot tell (cuCtxGetId, CUDA 12.0+).  The driver entry
+// points are fetched through the runtime, so the library does not link
+// libcuda itself.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    unsigned long long id = 0;
+    return get_id(c, &id) == CUDA_SUCCESS ? id : 0;
+}
+
+// Device address of the scratch on device `dev` (the current device): looked
+// up with that device current the first time, and again whenever the
+// device's context is not the one the cached address was found in.  When the
+// context id is unknown the address is looked up on every call.
 void *scratch_on_device(int dev)
 {
     std::lock_guard<std::mutex> lock(g_mu);
     if (dev < 0 || dev >= 64) return nullptr;
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            return nullptr;
-        }
-        g_scratch_addr[dev] = p;
+    ScratchAddr &a = g_scratch_addr[dev];
+    const unsigned long long ctx = current_context_id();
+    if (a.ptr && ctx != 0 && a.ctx == ctx) return a.ptr;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        return nullptr;
     }
-    return g_scratch_addr[dev];
+    a.ptr = p;
+    a.ctx = current_context_id();  // the lookup made the primary context current
+    return p;
 }
 
 }  // namespace

@@ -200,7 +200,8 @@ __global__ void __launch_bounds__(TW * 32, TiledShape<SIGMA>::MINB)
 tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__restrict__ blob,
              const int *__restrict__ tile_seg, const int *__restrict__ ne,
              const typename PT::V *__restrict__ x, double *__restrict__ y, double alpha,
-             double beta, double *__restrict__ carry_val, unsigned *status, int evict_first)
+             double beta, double *__restrict__ carry_val, unsigned *status, int evict_first,
+             int first_wait)
 {
     using V = typename PT::V;
     constexpr int TILE = 32 * SIGMA;
@@ -242,9 +243,13 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
     unsigned timeout = 0;
     uint32_t phases = 0u;  // bit b: parity of buffer b's next phase
     const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
-    auto wait_buf = [&](int bb) {
-        bool ok = mbar_wait(bar_base + 8 * bb, (phases >> bb) & 1u);
-        phases ^= 1u << bb;
+    // first_wait >= 0 (a test hook): the grid's first warp gives up its first
+    // wait after that many polls and takes the timeout path below.
+    int polls = first_wait >= 0 && blockIdx.x == 0 && warp == 0 ? first_wait : kWaitPolls;
+    auto wait_buf = [&](int bb) {  // the phase bit flips only once the copy has landed
+        const bool ok = mbar_wait(bar_base + 8 * bb, (phases >> bb) & 1u, polls);
+        polls = kWaitPolls;
+        if (ok) phases ^= 1u << bb;
         return ok;
     };
     int b = 0;
@@ -290,9 +295,12 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
         nb0 = nb0_n;
     }
     if (timeout) {
-        // let copies still in flight land (bounded) before the warp leaves
-#pragma unroll
-        for (int bb = 0; bb < NBUF; ++bb) mbar_wait(bar_base + 8 * bb, (phases >> bb) & 1u);
+        // Let every copy still in flight land (bounded) before the warp
+        // leaves: tile t in buffer b and the tiles t + k*W queued after it.
+        for (int k = 0; k < NBUF && t + k * W < tiles; ++k) {
+            const int bb = (b + k) % NBUF;
+            mbar_wait(bar_base + 8 * bb, (phases >> bb) & 1u);
+        }
         if (lane == 0) atomicOr(status, ST_TIMEOUT);
     }
     (void)status;
@@ -338,7 +346,8 @@ void launch_tiled_n(const TiledPlan &T, int m, int n, long long nnz, double alph
     int grid = (int)(want < cap ? want : cap);
     hook_start(s);
     kern<<<grid, TW * 32, smem, s>>>(m, n, nnz, T.tiles, T.blob, T.tile_seg, T.ne, x, y, alpha,
-                                     beta, T.carry_val, status, evict_first);
+                                     beta, T.carry_val, status, evict_first,
+                                     first_wait_budget());
     hook_stop(s);
 }
 
@@ -427,7 +436,7 @@ int tiled_build(Plan *p, cudaStream_t s)
     auto al = [&](void **ptr, size_t bytes) {
         bytes = bytes ? bytes : 16;
         p->scratch_bytes += bytes;
-        return cudaMallocAsync(ptr, bytes, s) == cudaSuccess;
+        return dev_malloc_async(ptr, bytes, s) == cudaSuccess;
     };
     const int m = p->m;
     int *flag = nullptr, *rank = nullptr;

@@ -62,10 +62,12 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
             : "memory");
 }
 // Bounded wait for the phase with the given parity; false if it never came
-// (the caller raises ST_TIMEOUT and stops instead of spinning for ever).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+// within `polls` tries (the caller raises ST_TIMEOUT and stops instead of
+// spinning for ever).
+constexpr int kWaitPolls = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int polls = kWaitPolls)
 {
-    for (int i = 0; i < (1 << 22); ++i) {
+    for (int i = 0; i < polls; ++i) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"

@@ -31,6 +31,15 @@ inline bool ranges_overlap(const void *a, size_t abytes, const void *b, size_t b
     return pa < pb + bbytes && pb < pa + abytes;
 }
 
+// ---- test hooks (hooks.cpp; armed only by sbb_test_hook) -------------------
+// cudaMallocAsync, except that an armed allocation-failure hook fails it.
+cudaError_t dev_malloc_async(void **p, size_t bytes, cudaStream_t s);
+// Free device memory as the drop-in memory pre-check sees it.
+size_t capped_free_bytes(size_t free_b);
+// -1, or the poll budget of the first tile-copy wait of a tiled launch's
+// first warp.
+int first_wait_budget();
+
 // Device status word bits, written by kernels instead of trapping.
 enum : unsigned {
     ST_BAD_ROWPTR = 1u << 0,   // non-monotone row pointer or out of [0, nnz]

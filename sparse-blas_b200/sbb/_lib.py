@@ -98,7 +98,11 @@ SIGNATURES = {
     "sbb_spmv_merge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_double, vp,
                                          C.c_double, vp, vp]),
     "sbb_last_error": (C.c_char_p, []),
+    "sbb_test_hook": (C.c_int, [C.c_int, C.c_longlong]),
 }
+
+# sbb_test_hook selectors (include/sbb_spmv.h)
+TEST_RESET, TEST_FAIL_ALLOC, TEST_FREE_BYTES, TEST_WAIT_BUDGET = 0, 1, 2, 3
 
 
 def lib():

@@ -148,3 +148,14 @@ def test_batch_and_tuner_reject_bad_arguments_on_the_host():
                                   None) == -1
     assert lib().sbb_batch_run(None, None) == -1
     assert lib().sbb_batch_destroy(None) == 0
+
+
+def test_test_hook_selectors():
+    """sbb_test_hook is host-only: it arms and disarms without a GPU and
+    refuses an unknown selector."""
+    from sbb._lib import TEST_FAIL_ALLOC, TEST_RESET, TEST_WAIT_BUDGET, lib
+    L = lib()
+    assert L.sbb_test_hook(99, 0) == -1
+    assert L.sbb_test_hook(TEST_FAIL_ALLOC, -1) == -1
+    assert L.sbb_test_hook(TEST_WAIT_BUDGET, 0) == 0
+    assert L.sbb_test_hook(TEST_RESET, 0) == 0
