@@ -46,6 +46,7 @@ sys.path.insert(0, os.path.join(ROOT, "sparse-blas_b200"))
 import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+KERNEL_TAGS = {1: "vector_kernel", 2: "merge_kernel", 3: "tiled_kernel", 5: "rows_kernel"}
 
 
 def algo_bytes(m, n, nnz):
@@ -264,17 +265,17 @@ def c5_matrices(count, dev):
     return mats, total
 
 
-def run_batch(args, ws, rank, local):
-    """c5: 512 matrices; per-matrix plain launches vs one graph launch of the
-    batch (a persistent kernel per kernel family, then the carry fix-up), with
-    the learned selector's, the heuristic's and the exhaustive autotuner's
-    classes.  ``value`` is the batch with the selector's classes."""
+def batch_measure(count, reps, local):
+    """c5: `count` matrices; per-matrix plain launches vs one graph launch of
+    the batch (a persistent kernel per kernel family, then the carry fix-up),
+    with the learned selector's, the heuristic's and the exhaustive
+    autotuner's classes.  Returns the measured figures (ms per batch, regrets,
+    class counts); the batch with the selector's classes is the headline."""
     import torch
     from sbb.batch import Batch, tune
     from sbb.selector import Selector
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    count = args.batch_count
     t_gen = time.perf_counter()
     mats, total_bytes = c5_matrices(count, dev)
     t_gen = time.perf_counter() - t_gen
@@ -306,14 +307,29 @@ def run_batch(args, ws, rank, local):
     res = {}
     for name, classes in (("mlp", mlp), ("default", default), ("tuned", best)):
         B = Batch(mats, classes)
-        res[f"each_{name}_ms"] = timed(B.run_each, args.batch_reps)
-        res[f"batch_{name}_ms"] = timed(B.run_graph, args.batch_reps)
+        res[f"each_{name}_ms"] = timed(B.run_each, reps)
+        res[f"batch_{name}_ms"] = timed(B.run_graph, reps)
         B.check()
         res[f"launches_each_{name}"] = B.launches(per_matrix=True)
         res[f"launches_batch_{name}"] = B.launches()
         B.close()
     best_sum = float(times.min(axis=1).sum())
     pick = lambda cls: float(sum(times[i, c] for i, c in enumerate(cls)))  # noqa: E731
+    flops = sum(2 * d["A"].nnz + 3 * d["m"] for d in mats)
+    del mats
+    torch.cuda.empty_cache()
+    return dict(res=res, total_bytes=total_bytes, flops=flops, t_gen=t_gen, t_tune=t_tune,
+                t_sel=t_sel, mlp=mlp, best=best, default=default,
+                regret_mlp=pick(mlp) / best_sum - 1, regret_default=pick(default) / best_sum - 1)
+
+
+def run_batch(args, ws, rank, local):
+    """c5 line: ``value`` is the batch with the selector's classes."""
+    count = args.batch_count
+    r = batch_measure(count, args.batch_reps, local)
+    res, total_bytes = r["res"], r["total_bytes"]
+    t_gen, t_tune, t_sel = r["t_gen"], r["t_tune"], r["t_sel"]
+    mlp, best, default = r["mlp"], r["best"], r["default"]
     ms = max_over_ranks(res["batch_mlp_ms"], ws)
     value = total_bytes * ws / (ms * 1e-3) / 1e9
     if rank != 0:
@@ -334,8 +350,8 @@ def run_batch(args, ws, rank, local):
                    "classes_default": np.bincount(default, minlength=6).tolist(),
                    "speedup_batch_vs_each_default": round(res["each_default_ms"] / ms, 3),
                    "speedup_batch_vs_each_mlp": round(res["each_mlp_ms"] / ms, 3),
-                   "regret_mlp": round(pick(mlp) / best_sum - 1, 4),
-                   "regret_default": round(pick(default) / best_sum - 1, 4),
+                   "regret_mlp": round(r["regret_mlp"], 4),
+                   "regret_default": round(r["regret_default"], 4),
                    **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in res.items()}},
         "gpu_launches": res["launches_batch_mlp"] * args.batch_reps,
     }
@@ -379,7 +395,7 @@ def run_reference_batch(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_f32(args, ws, rank, local):
+def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local):
     """FP32-storage compensated form vs the FP64 plan on the same matrix, both
     timed here (main kernel with CUDA events, whole steps), with max and
     median per-row error against the FP64 double-double oracle."""
@@ -392,25 +408,21 @@ def run_f32(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    A, x_h, y_h, alpha, beta, desc = make_workload(args.workload)
-    m, n, nnz = A.m, A.n, A.nnz
-    bytes64 = algo_bytes(m, n, nnz)
-    bytes32 = 8 * nnz + 4 * (m + 1) + 4 * n + 16 * m
+    n = A.n
     rp = torch.from_numpy(A.rowptr32()).to(dev)
     col = torch.from_numpy(A.col).to(dev)
     y0 = torch.from_numpy(y_h).to(dev)
-    kw = dict(tile_sigma=args.sigma) if args.kernel == "tiled" else {}
-    P64 = Plan(rp, col, torch.from_numpy(A.val).to(dev), n, kernel=args.kernel, **kw)
-    P32 = Plan(rp, col, torch.from_numpy(A.val.astype(np.float32)).to(dev), n, kernel=args.kernel,
+    P64 = Plan(rp, col, torch.from_numpy(A.val).to(dev), n, kernel=kernel, **kw)
+    P32 = Plan(rp, col, torch.from_numpy(A.val.astype(np.float32)).to(dev), n, kernel=kernel,
                f32=True, **kw)
     x64 = torch.from_numpy(x_h).to(dev)
     x32 = torch.from_numpy(x_h.astype(np.float32)).to(dev)
     stream = torch.cuda.current_stream()
     sp = C.c_void_p(stream.cuda_stream)
 
-    def timed(P, x, steps):
+    def timed(P, x):
         y = y0.clone()
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             P.spmv(x, y, alpha, beta)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps + 2)]
         for e in ev:
@@ -425,23 +437,40 @@ def run_f32(args, ws, rank, local):
         ev[1].record(stream)
         torch.cuda.synchronize()
         P.check()
-        kern = statistics.mean(ev[2 + 2 * i].elapsed_time(ev[3 + 2 * i]) for i in range(steps))
+        kern = statistics.median(ev[2 + 2 * i].elapsed_time(ev[3 + 2 * i]) for i in range(steps))
         return ev[0].elapsed_time(ev[1]) / steps, kern
 
-    with ClockSampler(local) as clk:
-        step64, kern64 = timed(P64, x64, args.steps)
-        step32, kern32 = timed(P32, x32, args.steps)
-    ms32 = max_over_ranks(step32, ws)
+    step64, kern64 = timed(P64, x64)
+    step32, kern32 = timed(P32, x32)
     y = y0.clone()
     P32.spmv(x32, y, alpha, beta)
     torch.cuda.synchronize()
     got = y.cpu().numpy()
     ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x_h, alpha, beta, y_h)
     err = np.abs(got - ref) / np.where(sc > 0, sc, 1.0)
-    tag = {1: "vector_kernel", 2: "merge_kernel", 3: "tiled_kernel"}[P32.info()["kernel"]]
+    info = P32.info()
+    launches = lib().sbb_plan_launches(P32.h)
+    P64.close()
+    P32.close()
+    return dict(step64=step64, kern64=kern64, step32=step32, kern32=kern32,
+                err_max=float(err.max()), err_median=float(np.median(err)), info=info,
+                launches=launches,
+                tag=KERNEL_TAGS[info["kernel"]])
+
+
+def run_f32(args, ws, rank, local):
+    """FP32-storage form line (``--f32``)."""
+    A, x_h, y_h, alpha, beta, desc = make_workload(args.workload)
+    m, n, nnz = A.m, A.n, A.nnz
+    bytes64 = algo_bytes(m, n, nnz)
+    bytes32 = 8 * nnz + 4 * (m + 1) + 4 * n + 16 * m
+    kw = dict(tile_sigma=args.sigma) if args.kernel == "tiled" else {}
+    with ClockSampler(local) as clk:
+        r = f32_measure(A, x_h, y_h, alpha, beta, args.kernel, kw, args.warmup, args.steps, local)
+    ms32 = max_over_ranks(r["step32"], ws)
     peak, peak_kind = peaks()
     if rank == 0:
-        ach = bytes32 / (kern32 * 1e-3) / 1e9
+        ach = bytes32 / (r["kern32"] * 1e-3) / 1e9
         print(json.dumps({
             "metric": "SpMV GB/s, FP32-storage compensated form (algorithmic bytes "
                       "8*nnz+4*(m+1)+4*n+16*m)",
@@ -450,23 +479,22 @@ def run_f32(args, ws, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": desc + " (val and x rounded to FP32, y FP64)", "m": m, "n": n,
-                       "nnz": nnz, "kernel": tag, "plan": {k: P32.info()[k] for k in
-                                                           ("tile_sigma", "vector_width",
-                                                            "items_per_thread")},
-                       "fp64_plan_ms_per_step": round(step64, 5),
-                       "fp64_kernel_ms": round(kern64, 5), "f32_kernel_ms": round(kern32, 5),
-                       "speedup_step_vs_fp64": round(step64 / step32, 3),
-                       "speedup_kernel_vs_fp64": round(kern64 / kern32, 3),
+                       "nnz": nnz, "kernel": r["tag"], "plan": {k: r["info"][k] for k in
+                                                                ("tile_sigma", "vector_width",
+                                                                 "items_per_thread")},
+                       "fp64_plan_ms_per_step": round(r["step64"], 5),
+                       "fp64_kernel_ms": round(r["kern64"], 5),
+                       "f32_kernel_ms": round(r["kern32"], 5),
+                       "speedup_step_vs_fp64": round(r["step64"] / r["step32"], 3),
+                       "speedup_kernel_vs_fp64": round(r["kern64"] / r["kern32"], 3),
                        "byte_ratio": round(bytes64 / bytes32, 3),
-                       "err_max": float(err.max()), "err_median": float(np.median(err)),
+                       "err_max": r["err_max"], "err_median": r["err_median"],
                        "err_metric": "|y - y_oracle| / (|alpha| sum|a x| + |beta y|), FP64 "
                                      "double-double oracle on the FP64 inputs"},
             "roofline": {"bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 4), "traffic": None, "peak_source": peak_kind},
-            "gpu_launches": lib().sbb_plan_launches(P32.h) * args.steps,
+            "gpu_launches": r["launches"] * args.steps,
             "clocks": clk.summary()}), flush=True)
-    P64.close()
-    P32.close()
 
 
 def library_spmv(args, m, n, rp, col, val, x, y0, alpha, beta, bytes_step):
@@ -502,6 +530,123 @@ def library_spmv(args, m, n, rp, col, val, x, y0, alpha, beta, bytes_step):
         return out
     except Exception as e:  # a comparator only: its absence does not fail the bench
         return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
+def plain_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, reps, local):
+    """One plain plan on a resident matrix: the plan's build time (a second
+    build, after the modules are loaded), the main kernel's median time and
+    whole steps (kernel + carry fix-up), each over `reps` launches."""
+    import ctypes as C
+    import torch
+    from sbb._lib import lib
+    from sbb.device import Plan
+    dev = torch.device("cuda", local)
+    rp = torch.from_numpy(A.rowptr32()).to(dev)
+    col = torch.from_numpy(A.col).to(dev)
+    val = torch.from_numpy(A.val).to(dev)
+    x = torch.from_numpy(x_h).to(dev)
+    y = torch.from_numpy(y_h).to(dev)
+    Plan(rp, col, val, A.n, kernel=kernel, **kw).close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    P = Plan(rp, col, val, A.n, kernel=kernel, **kw)
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    for _ in range(warmup):
+        P.spmv(x, y, alpha, beta)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps + 2)]
+    for e in ev:
+        e.record(stream)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for i in range(reps):
+        assert lib().sbb_spmv_timed(P.h, alpha, C.c_void_p(x.data_ptr()), beta,
+                                    C.c_void_p(y.data_ptr()), sp,
+                                    C.c_void_p(ev[2 + 2 * i].cuda_event),
+                                    C.c_void_p(ev[3 + 2 * i].cuda_event)) == 0
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    P.check()
+    kern = statistics.median(ev[2 + 2 * i].elapsed_time(ev[3 + 2 * i]) for i in range(reps))
+    step = ev[0].elapsed_time(ev[1]) / reps
+    info = P.info()
+    launches = lib().sbb_plan_launches(P.h)
+    P.close()
+    return dict(kernel_ms=kern, step_ms=step, plan_build_ms=build_ms, info=info,
+                launches=launches)
+
+
+def config_line(name, kernel, kw, local, cpu_budget, reps=200):
+    """Sub-object of the default line for another benchmark configuration:
+    GB/s and GFLOP/s of the step and of the main kernel, the fraction of the
+    HBM peak, and the reference's host loop on the same matrix."""
+    A, x_h, y_h, alpha, beta, desc = make_workload(name)
+    r = plain_measure(A, x_h, y_h, alpha, beta, kernel, kw, 10, reps, local)
+    b = algo_bytes(A.m, A.n, A.nnz)
+    fl = 2 * A.nnz + 3 * A.m
+    peak, peak_kind = peaks()
+    threads = os.cpu_count() or 1
+    sec, cpu_reps = cpu_sample_time(A, x_h, y_h, alpha, beta, threads, budget_s=cpu_budget)
+    tag = KERNEL_TAGS[r["info"]["kernel"]]
+    return {"workload": desc, "m": A.m, "n": A.n, "nnz": A.nnz, "kernel": tag,
+            "plan": {k: r["info"][k] for k in ("vector_width", "items_per_thread",
+                                               "tile_sigma", "tiles")},
+            "step_ms": round(r["step_ms"], 5), "kernel_ms": round(r["kernel_ms"], 5),
+            "GB/s": round(b / (r["step_ms"] * 1e-3) / 1e9, 2),
+            "GFLOP/s": round(fl / (r["step_ms"] * 1e-3) / 1e9, 2),
+            "kernel_GB/s": round(b / (r["kernel_ms"] * 1e-3) / 1e9, 2),
+            "frac": round(b / (r["kernel_ms"] * 1e-3) / 1e9 / peak, 4), "peak": peak,
+            "peak_source": peak_kind, "algorithmic_bytes": b, "flops": fl,
+            "plan_build_ms": round(r["plan_build_ms"], 3), "reps": reps,
+            "gpu_launches": r["launches"] * reps,
+            "cpu_host_loop": {"GB/s": round(b / sec / 1e9, 3), "cores": threads,
+                              "sample": f"{cpu_reps} full passes"}}
+
+
+def extra_configs(A2, x2, y2, local, cpu_budget):
+    """The other benchmark configurations, measured after the timed region of
+    the default line (one GPU): c1 and c3 plain, the FP32-storage form on the
+    c1 and c2 matrices (c4), and the 512-matrix batch with the learned
+    selector (c5)."""
+    out = {}
+    out["c1"] = config_line("c1", "auto", {}, local, min(cpu_budget, 2.0), reps=500)
+    out["c3"] = config_line("c3", "auto", {}, local, min(cpu_budget, 3.0), reps=100)
+    f = {}
+    for name, (A, x_h, y_h, alpha, beta) in (("c1_matrix", make_workload("c1")[:5]),
+                                             ("c2_matrix", (A2, x2, y2, 1.0, 0.5))):
+        r = f32_measure(A, x_h, y_h, alpha, beta, "auto", {}, 10, 100, local)
+        b64 = algo_bytes(A.m, A.n, A.nnz)
+        b32 = 8 * A.nnz + 4 * (A.m + 1) + 4 * A.n + 16 * A.m
+        f[name] = {"kernel": r["tag"], "fp64_kernel_ms": round(r["kern64"], 5),
+                   "f32_kernel_ms": round(r["kern32"], 5),
+                   "fp64_step_ms": round(r["step64"], 5), "f32_step_ms": round(r["step32"], 5),
+                   "speedup_kernel_vs_fp64": round(r["kern64"] / r["kern32"], 3),
+                   "speedup_step_vs_fp64": round(r["step64"] / r["step32"], 3),
+                   "f32_GB/s": round(b32 / (r["step32"] * 1e-3) / 1e9, 2),
+                   "f32_GFLOP/s": round((2 * A.nnz + 3 * A.m) / (r["step32"] * 1e-3) / 1e9, 2),
+                   "byte_ratio": round(b64 / b32, 3),
+                   "err_max": r["err_max"], "err_median": r["err_median"]}
+    f["err_metric"] = ("|y - y_oracle| / (|alpha| sum|a x| + |beta y|) against the FP64 "
+                       "double-double oracle on the FP64 inputs")
+    out["f32"] = f
+    r = batch_measure(512, 10, local)
+    res = r["res"]
+    ms = res["batch_mlp_ms"]
+    out["c5"] = {"workload": C5_DESC.format(count=512),
+                 "batch_ms": round(ms, 4), "each_ms": round(res["each_default_ms"], 4),
+                 "speedup_batch_vs_each": round(res["each_default_ms"] / ms, 3),
+                 "batch_tuned_ms": round(res["batch_tuned_ms"], 4),
+                 "batch_default_ms": round(res["batch_default_ms"], 4),
+                 "GB/s": round(r["total_bytes"] / (ms * 1e-3) / 1e9, 2),
+                 "GFLOP/s": round(r["flops"] / (ms * 1e-3) / 1e9, 2),
+                 "regret_mlp": round(r["regret_mlp"], 4),
+                 "regret_default": round(r["regret_default"], 4),
+                 "launches_batch": res["launches_batch_mlp"],
+                 "launches_each": res["launches_each_default"],
+                 "baseline": "each matrix's own plain launches with the heuristic's classes"}
+    return out
 
 
 def run_sbb(args, ws, rank, local):
@@ -569,7 +714,7 @@ def run_sbb(args, ws, rank, local):
     value = ws * bytes_step / (ms_step * 1e-3) / 1e9
     peak, peak_kind = peaks()
     achieved = bytes_step / (kern_avg * 1e-3) / 1e9
-    tag = {1: "vector_kernel", 2: "merge_kernel", 3: "tiled_kernel"}[info["kernel"]]
+    tag = KERNEL_TAGS[info["kernel"]]
     traffic = traffic_from_profile(tag, args.workload) if not args.workload.startswith("mtx:") else None
 
     # e2e through the reference-facing C ABI with pinned host buffers
@@ -610,6 +755,46 @@ def run_sbb(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_library:
         library = library_spmv(args, m, n, rp, col, val, x, y0, alpha, beta, bytes_step)
 
+    # one-time costs: the plan build (a second build of the same plan) and the
+    # reference-named csr5_kernel, which builds and drops a tile plan per call
+    build = None
+    if rank == 0 and ws == 1:
+        torch.cuda.synchronize()
+        t_b = time.perf_counter()
+        P2 = Plan(rp, col, val, n, kernel=args.kernel, **kw)
+        torch.cuda.synchronize()
+        build_ms = (time.perf_counter() - t_b) * 1e3
+        P2.close()
+        a_c, b_c = C.c_double(alpha), C.c_double(beta)
+        yc = y0.clone()
+        csr5 = []
+        for _ in range(4):
+            torch.cuda.synchronize()
+            t_c = time.perf_counter()
+            rc = lib().csr5_kernel(m, n, nnz, C.byref(a_c), C.c_void_p(val.data_ptr()),
+                                   C.c_void_p(rp.data_ptr()), C.c_void_p(col.data_ptr()),
+                                   C.c_void_p(x.data_ptr()), C.byref(b_c),
+                                   C.c_void_p(yc.data_ptr()))
+            torch.cuda.synchronize()
+            csr5.append((time.perf_counter() - t_c) * 1e3)
+            assert rc == 0
+        build = {"plan_build_ms": round(build_ms, 3),
+                 "break_even_spmv_vs_cusparse_alg1": (
+                     round(build_ms / (library["alg1"]["ms_per_call"] - ms_step), 1)
+                     if library and "alg1" in library
+                     and library["alg1"]["ms_per_call"] > ms_step else None),
+                 "csr5_kernel_ms_per_call": round(statistics.median(csr5[1:]), 3),
+                 "note": "plan_build_ms: host wall time of a second sbb_plan_create of the "
+                         "timed plan (row-pointer check, tile format, carry lists); "
+                         "csr5_kernel (device pointers) builds, runs and drops a tile plan "
+                         "in every call, as the reference converts to CSR5 in every call"}
+
+    extra = {}
+    if rank == 0 and ws == 1 and args.workload == "c2" and not args.no_extra:
+        with ClockSampler(local) as clk2:
+            extra = extra_configs(A, x_h, y_h, local, args.cpu_budget)
+        extra["extra_clocks"] = clk2.summary()
+
     if rank == 0:
         line = {
             "metric": "SpMV HBM GB/s (FP64 CSR, algorithmic bytes 12*nnz+4*(m+1)+8*n+16*m)",
@@ -631,6 +816,8 @@ def run_sbb(args, ws, rank, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "library_spmv": library,
+            "one_time": build,
+            **extra,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
         }
@@ -648,7 +835,8 @@ def main():
     ap.add_argument("--mtx", default=None, help="benchmark a Matrix Market file instead")
     ap.add_argument("--batch-count", type=int, default=512, help="c5: matrices in the batch")
     ap.add_argument("--batch-reps", type=int, default=20, help="c5: timed batch runs")
-    ap.add_argument("--kernel", default="tiled", choices=["merge", "vector", "tiled", "auto"])
+    ap.add_argument("--kernel", default="tiled",
+                    choices=["merge", "vector", "tiled", "rows", "auto"])
     ap.add_argument("--ipt", type=int, default=6)
     ap.add_argument("--persistent", type=int, default=0)
     ap.add_argument("--sigma", type=int, default=4, help="tiled kernel: nnz per lane (0 = CSR5 rule)")
@@ -657,6 +845,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-library", action="store_true",
                     help="skip the cuSPARSE comparator (library_spmv key)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="c2: skip the c1 / c3 / FP32 / c5 sub-objects")
     ap.add_argument("--f32", action="store_true",
                     help="time the FP32-storage compensated form against the FP64 plan")
     args = ap.parse_args()

@@ -87,11 +87,18 @@ enum {
     SBB_KERNEL_VECTOR = 1, /* K1: V lanes per row, warp-shuffle reduce   */
     SBB_KERNEL_MERGE = 2,  /* K2: merge-path split of rows+nnz over CTAs */
     SBB_KERNEL_TILED = 3,  /* K3: CSR5-style 32 x sigma tiles            */
-    SBB_KERNEL_LEARNED = 4 /* the trained selector (sbb_mlp_select, built-in
+    SBB_KERNEL_LEARNED = 4,/* the trained selector (sbb_mlp_select, built-in
                               parameters) picks one of the SBB_NUM_CLASSES
                               batch classes' configurations on the GPU; the
                               parameters (21.6 KB) are copied to a device
                               the first time it is used and kept until exit */
+    SBB_KERNEL_ROWS = 5    /* K4: blocks of <= 32 rows and <= 384 nnz (rows
+                              longer than 384 nnz split into pieces), staged
+                              into shared memory by TMA straight from the
+                              caller's CSR arrays (no copy of the matrix),
+                              one lane per row; no counterpart in the
+                              reference.  Needs 4-byte-aligned int arrays and
+                              an 8-byte-aligned (FP32: 4) value array. */
 };
 
 typedef struct {

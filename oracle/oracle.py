@@ -42,6 +42,8 @@ class Slice(C.Structure):
 
 
 def build(ref: bool = False) -> None:
+    """liboracle.so; with ref, also _ref/libref.so from the reference sources
+    named by REF or SBB_REFERENCE_SRC in the environment."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)

@@ -30,6 +30,10 @@ int plan_launches(const Plan *p)
         extern int tiled_launches(const Plan *);
         return tiled_launches(p);
     }
+    case SBB_KERNEL_ROWS: {
+        extern int rows_launches(const Plan *);
+        return rows_launches(p);
+    }
     default: return 0;
     }
 }
@@ -118,6 +122,8 @@ void plan_free_async(Plan *p, cudaStream_t s)
     carry_runs_free(&p->runs, s, true);
     extern void tiled_free_async(Plan *, cudaStream_t);
     tiled_free_async(p, s);
+    extern void rows_free_async(Plan *, cudaStream_t);
+    rows_free_async(p, s);
     p->tile_row = p->tile_nnz = nullptr;
     p->carry_val = nullptr;
     p->queue = p->status = nullptr;
@@ -131,6 +137,8 @@ void plan_free(Plan *p)
     carry_runs_free(&p->runs, 0, false);
     extern void tiled_free(Plan *);
     tiled_free(p);
+    extern void rows_free(Plan *);
+    rows_free(p);
     p->tile_row = p->tile_nnz = nullptr;
     p->carry_val = nullptr;
     p->queue = p->status = nullptr;
@@ -139,6 +147,9 @@ void plan_free(Plan *p)
 extern int tiled_build(Plan *p, cudaStream_t s);
 extern int tiled_run(Plan *p, double alpha, const void *x, double beta, double *y,
                      cudaStream_t s);
+extern int rows_build(Plan *p, cudaStream_t s);
+extern int rows_run(Plan *p, double alpha, const void *x, double beta, double *y,
+                    cudaStream_t s);
 
 // Build scratch for the resolved kernel.  Validation (one sync) only when
 // `validate`; the drop-in validates while narrowing the row pointer instead.
@@ -259,6 +270,21 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
         }
         return SBB_OK;
     }
+    if (k == SBB_KERNEL_ROWS) {
+        rc = rows_build(p, s);
+        if (rc != SBB_OK) return rc;
+        SBB_CUDA(cudaGetLastError());
+        if (validate) {  // the plan range-checked every column
+            unsigned st = 0;
+            SBB_CUDA(cudaMemcpyAsync(&st, p->status, sizeof(st), cudaMemcpyDeviceToHost, s));
+            SBB_CUDA(cudaStreamSynchronize(s));
+            if (st & ST_BAD_COL) {
+                set_error("column index out of range [0, n)");
+                return SBB_ERR_INPUT;
+            }
+        }
+        return SBB_OK;
+    }
     set_error("unknown kernel id");
     return SBB_ERR_ARG;
 }
@@ -299,6 +325,8 @@ int plan_run(Plan *p, double alpha, const void *x, double beta, double *y, cudaS
     }
     case SBB_KERNEL_TILED:
         return tiled_run(p, alpha, x, beta, y, s);
+    case SBB_KERNEL_ROWS:
+        return rows_run(p, alpha, x, beta, y, s);
     default:
         set_error("plan has no kernel");
         return SBB_ERR_ARG;

@@ -232,6 +232,7 @@ struct Plan {
     unsigned *status = nullptr;
     int tiles = 0, persistent_ctas = 0;
     void *tiled = nullptr;   // K3 tile plan (k_tiled.cu)
+    void *rows = nullptr;    // K4 row-block plan (k_rows.cu)
     size_t scratch_bytes = 0;
     int device = 0;
 };

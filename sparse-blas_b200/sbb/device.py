@@ -9,7 +9,7 @@ import ctypes as C
 
 from ._lib import Config, PlanInfo, last_error, lib
 
-KERNELS = {"auto": 0, "vector": 1, "merge": 2, "tiled": 3, "learned": 4}
+KERNELS = {"auto": 0, "vector": 1, "merge": 2, "tiled": 3, "learned": 4, "rows": 5}
 
 
 class SbbError(RuntimeError):

@@ -1,7 +1,8 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
 Run in the development container, where oracle/_ref/libref.so can be built
-from the reference sources (``make -C oracle ref``).  That library is the
+from the reference sources (``make -C oracle ref REF=<its SparseBLAS
+directory>``, or with SBB_REFERENCE_SRC set).  That library is the
 reference's host drivers (SparseBLAS/src/dspmv_mgpu_{baseline,v1,v2}.cu and
 spmv_helper.cu), compiled unchanged against CPU stand-ins for the CUDA runtime
 and the removed legacy cuSPARSE csrmv (oracle/ref_shim.cpp).  Each fixture

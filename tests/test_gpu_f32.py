@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 
 CONFIGS = [dict(kernel="vector", vector_width=v) for v in (4, 16, 32)] + \
           [dict(kernel="merge", items_per_thread=i) for i in (4, 8)] + \
-          [dict(kernel="tiled", tile_sigma=s) for s in (4, 8, 16, 32)] + [dict(kernel="auto")]
+          [dict(kernel="tiled", tile_sigma=s) for s in (4, 8, 16, 32)] + [dict(kernel="rows")] + \
+          [dict(kernel="auto")]
 
 MATS = {
     "uniform": lambda: rand_csr(11, 5000, 4000, 0, 30),
@@ -64,14 +65,16 @@ def test_f32_form_within_tolerance(cuda, cfg, mat):
     assert e32 <= 1e-12, e32
 
 
+@pytest.mark.parametrize("kernel", ["tiled", "rows"])
 @pytest.mark.parametrize("which", ["c1", "c2"])
-def test_f32_form_on_benchmark_matrices(cuda, which):
+def test_f32_form_on_benchmark_matrices(cuda, which, kernel):
     """The C4 configuration (the 10k power-law matrix in FP32 storage) and the
-    5.5M-row irregular matrix, tiled kernel: max and median per-row error."""
+    5.5M-row irregular matrix, tiled and row-block kernels: max and median
+    per-row error."""
     from sbb import gen
     A = gen.c1() if which == "c1" else gen.c2()
     x = gen.uniform_vec(11 if which == "c1" else 21, A.n)
     y = gen.uniform_vec(22, A.m) if which == "c2" else np.zeros(A.m)
     beta = 0.5 if which == "c2" else 0.0
-    e64, e32 = check(A.rowptr, A.col, A.val, x, y, A.n, 1.0, beta, dict(kernel="tiled"))
+    e64, e32 = check(A.rowptr, A.col, A.val, x, y, A.n, 1.0, beta, dict(kernel=kernel))
     assert e64 <= TOL_FP32 and e32 <= 1e-12, (e64, e32)

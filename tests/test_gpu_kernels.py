@@ -16,7 +16,7 @@ CONFIGS = [dict(kernel="vector", vector_width=v) for v in (2, 4, 8, 16, 32)] + \
           [dict(kernel="merge", items_per_thread=i) for i in (4, 6, 8, 12)] + \
           [dict(kernel="merge", items_per_thread=8, persistent=p) for p in (1, 2, 4)] + \
           [dict(kernel="tiled"), dict(kernel="tiled", tile_sigma=4), dict(kernel="tiled", tile_sigma=16),
-           dict(kernel="auto")]
+           dict(kernel="rows"), dict(kernel="auto")]
 
 
 def to_dev(rp, col, val, x, y, f32=False):
@@ -84,7 +84,8 @@ def test_merge_partition_bit_exact(cuda, ipt, mat):
 
 @pytest.mark.parametrize("cfg", [dict(kernel="merge", items_per_thread=8),
                                  dict(kernel="merge", items_per_thread=8, persistent=2),
-                                 dict(kernel="vector", vector_width=8), dict(kernel="tiled")])
+                                 dict(kernel="vector", vector_width=8), dict(kernel="tiled"),
+                                 dict(kernel="rows")])
 def test_repeat_runs_bit_identical(cuda, cfg):
     rp, col, val, x, y = MATS["long_rows"]()
     outs, _ = run_plan(rp, col, val, x, y, len(x), 1.3, 0.4, cfg, reps=3)
@@ -105,15 +106,17 @@ def test_bad_column_is_flagged_not_faulted(cuda):
     P.close()
 
 
-def test_bad_column_rejected_by_tiled_plan(cuda):
-    """The tiled kernel range-checks columns once, when its plan copies them."""
+@pytest.mark.parametrize("kernel", ["tiled", "rows"])
+def test_bad_column_rejected_by_plan(cuda, kernel):
+    """The tiled and row-block kernels range-check columns once, when their
+    plan is built."""
     from sbb.device import Plan, SbbError
     rp, col, val, x, y = MATS["uniform"]()
     col = col.copy()
     col[-1] = -3
     drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
     with pytest.raises(SbbError):
-        Plan(drp, dcol, dval, len(x), kernel="tiled")
+        Plan(drp, dcol, dval, len(x), kernel=kernel)
 
 
 
@@ -125,7 +128,8 @@ def test_overlapping_x_and_y_rejected(cuda):
     rp, col, val, x, y = MATS["uniform"]()  # 5000 x 4000
     drp, dcol, dval, _, _ = to_dev(rp, col, val, x, y)
     buf = torch.zeros(9000, dtype=torch.float64, device="cuda")
-    for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="merge"), dict(kernel="tiled")):
+    for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="merge"), dict(kernel="tiled"),
+                dict(kernel="rows")):
         P = Plan(drp, dcol, dval, 4000, **cfg)
         with pytest.raises(SbbError):
             P.spmv(buf[:4000], buf[3999:8999], 1.0, 0.0)
@@ -153,7 +157,7 @@ def test_config1_full_parity(cuda):
     y = np.zeros(A.m)
     y_ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x, 1.0, 0.0, y)
     for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="merge"), dict(kernel="tiled"),
-                dict(kernel="auto")):
+                dict(kernel="rows"), dict(kernel="auto")):
         (out,), _ = run_plan(A.rowptr, A.col, A.val, x, y, A.n, 1.0, 0.0, cfg)
         assert max_scaled_err(out, y_ref, sc) <= TOL_FP64
 
@@ -167,7 +171,8 @@ def test_full_size_parity(cuda, which):
     y = gen.uniform_vec(22, A.m)
     beta = 0.5 if which == "c2" else 0.0
     y_ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x, 1.0, beta, y)
-    for cfg in (dict(kernel="merge", items_per_thread=8), dict(kernel="tiled"), dict(kernel="auto")):
+    for cfg in (dict(kernel="merge", items_per_thread=8), dict(kernel="tiled"), dict(kernel="rows"),
+                dict(kernel="auto")):
         (out,), _ = run_plan(A.rowptr, A.col, A.val, x, y, A.n, 1.0, beta, cfg)
         assert max_scaled_err(out, y_ref, sc) <= TOL_FP64, cfg
 
@@ -241,7 +246,7 @@ def test_column_indices_up_to_int32_max(cuda):
     dy0 = torch.from_numpy(W["y0"]).to(d)
     for cfg in (dict(kernel="vector", vector_width=8), dict(kernel="vector", vector_width=32),
                 dict(kernel="merge", items_per_thread=8), dict(kernel="tiled", tile_sigma=4),
-                dict(kernel="tiled", tile_sigma=16), dict(kernel="auto")):
+                dict(kernel="tiled", tile_sigma=16), dict(kernel="rows"), dict(kernel="auto")):
         P = Plan(drp, dcol, dval, n, **cfg)
         yy = dy0.clone()
         P.spmv(x, yy, alpha, beta)
@@ -250,13 +255,14 @@ def test_column_indices_up_to_int32_max(cuda):
         P.close()
         assert np.array_equal(yy.cpu().numpy(), want), cfg
     x32 = x.float()
-    P = Plan(drp, dcol, dval.float(), n, kernel="tiled", f32=True)
-    yy = dy0.clone()
-    P.spmv(x32, yy, alpha, beta)
-    torch.cuda.synchronize()
-    P.check()
-    P.close()
-    assert np.array_equal(yy.cpu().numpy(), want), "f32"
+    for kernel in ("tiled", "rows"):
+        P = Plan(drp, dcol, dval.float(), n, kernel=kernel, f32=True)
+        yy = dy0.clone()
+        P.spmv(x32, yy, alpha, beta)
+        torch.cuda.synchronize()
+        P.check()
+        P.close()
+        assert np.array_equal(yy.cpu().numpy(), want), ("f32", kernel)
     del x32, x
     torch.cuda.empty_cache()
 
@@ -328,7 +334,7 @@ def test_nnz_at_int32_max(cuda):
     W = _max_nnz_matrix(cuda)
     for cfg in (dict(kernel="vector", vector_width=32), dict(kernel="vector", vector_width=4),
                 dict(kernel="merge", items_per_thread=8), dict(kernel="tiled", tile_sigma=4),
-                dict(kernel="auto")):
+                dict(kernel="rows"), dict(kernel="auto")):
         P = Plan(W["rp"], W["col"], W["val"], W["n"], **cfg)
         yy = W["y0"].clone()
         P.spmv(W["x"], yy, W["alpha"], W["beta"])
@@ -400,7 +406,7 @@ def test_rows_at_int32_max(cuda):
     want.mul_(alpha).add_(y0, alpha=beta)
     yy = torch.empty_like(y0)
     for cfg in (dict(kernel="vector", vector_width=4), dict(kernel="merge", items_per_thread=8),
-                dict(kernel="auto")):
+                dict(kernel="rows"), dict(kernel="auto")):
         P = Plan(rp, col, val, n, **cfg)
         if cfg["kernel"] == "auto":
             assert P.info()["kernel"] == 2  # the merge path
@@ -412,3 +418,44 @@ def test_rows_at_int32_max(cuda):
         assert torch.equal(yy, want), cfg
     with pytest.raises(SbbError):
         Plan(rp, col, val, n, kernel="tiled")
+
+
+@pytest.mark.parametrize("f32", [False, True])
+def test_unaligned_views(cuda, f32):
+    """Row pointer, columns and values that are views at every element offset
+    of a 16-byte block of larger buffers: the row-block kernel copies only the
+    16-byte-aligned middle of each range by TMA and loads the ragged ends
+    itself, so each offset must give the oracle's result (and every kernel
+    must work on such views)."""
+    import torch
+    from sbb.device import Plan
+    rp, col, val, x, y = rand_csr(8, 3000, 2500, 0, 40, p_empty=0.1,
+                                  long_rows=[(7, 1000), (1500, 2400)])
+    d = torch.device("cuda:0")
+    vt = torch.float32 if f32 else torch.float64
+    nnz, m = len(col), len(rp) - 1
+    dx = torch.from_numpy(x).to(d, vt)
+    xs = dx.double().cpu().numpy() if f32 else x
+    vs = val.astype(np.float32).astype(np.float64) if f32 else val
+    y_ref, sc = O.spmv_dd(rp, col, vs, xs, 1.1, -0.6, y)
+    per16 = 4 if f32 else 2
+    for off_i in range(4):
+        for off_v in range(per16):
+            brp = torch.zeros(m + 1 + 8, dtype=torch.int32, device=d)
+            bcol = torch.zeros(nnz + 8, dtype=torch.int32, device=d)
+            bval = torch.zeros(nnz + 8, dtype=vt, device=d)
+            brp[off_i:off_i + m + 1] = torch.from_numpy(rp.astype(np.int32)).to(d)
+            bcol[(3 - off_i):(3 - off_i) + nnz] = torch.from_numpy(col).to(d)
+            bval[off_v:off_v + nnz] = torch.from_numpy(val).to(d, vt)
+            drp = brp[off_i:off_i + m + 1]
+            dcol = bcol[(3 - off_i):(3 - off_i) + nnz]
+            dval = bval[off_v:off_v + nnz]
+            for kernel in ("rows", "merge", "tiled", "vector"):
+                P = Plan(drp, dcol, dval, len(x), kernel=kernel, f32=f32)
+                yy = torch.from_numpy(y).to(d)
+                P.spmv(dx, yy, 1.1, -0.6)
+                torch.cuda.synchronize()
+                P.check()
+                P.close()
+                tol = 1e-12 if not f32 else 1e-12
+                assert max_scaled_err(yy.cpu().numpy(), y_ref, sc) <= tol, (kernel, off_i, off_v)
