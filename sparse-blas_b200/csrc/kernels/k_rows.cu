@@ -85,11 +85,12 @@ __device__ __forceinline__ Span span_of(const void *a, long long k0, long long k
 // of a long row (it writes y), or -1 for another piece (it leaves a carry);
 // z, w = nnz range [k0, k1) (absolute offsets, as the row pointer holds them).
 template <typename PT>
-__global__ void __launch_bounds__(RW * 32, 1)
+__global__ void __launch_bounds__(RW * 32, 5)
 rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
             const int *__restrict__ col, const typename PT::V *__restrict__ val,
             const typename PT::V *__restrict__ x, double *__restrict__ y, double alpha,
-            double beta, double *__restrict__ carry_val, unsigned *status, int first_wait)
+            double beta, double *__restrict__ carry_val, unsigned *status, int first_wait,
+            int m, int base, int nnz)
 {
     using V = typename PT::V;
     using S = RowsSlot<V>;
@@ -105,74 +106,121 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
     int b = blockIdx.x * RW + warp;
     uint64_t pol = 0;
 
-    // lane 0: the bulk copies of block d into slot sl
+    // The three ranges of block d as 4-byte words: g = 0 columns, 1 values,
+    // 2 row pointers (none for a piece of a long row).
+    struct Range {
+        const unsigned *a;
+        long long k0, n;
+        uint32_t off;  // slot region
+    };
+    auto range_of = [&](int4 d, int g) {
+        constexpr int VW = (int)sizeof(V) / 4;  // words per value
+        Range r;
+        r.a = g == 0 ? reinterpret_cast<const unsigned *>(col)
+                     : (g == 1 ? reinterpret_cast<const unsigned *>(val)
+                               : reinterpret_cast<const unsigned *>(rp));
+        r.k0 = g == 0 ? (long long)d.z : (g == 1 ? (long long)d.z * VW : (long long)d.x);
+        r.n = g == 0 ? (long long)d.w - d.z
+                     : (g == 1 ? ((long long)d.w - d.z) * VW : (d.y > 0 ? (long long)d.y + 1 : 0));
+        r.off = g == 0 ? S::C_OFF : (g == 1 ? S::V_OFF : S::R_OFF);
+        return r;
+    };
+    // The range of the matrix's own words an array may be read in (the
+    // view: nnz from `base`, rows 0..m), as byte addresses.
+    auto view_of = [&](int g, uintptr_t &vlo, uintptr_t &vhi) {
+        constexpr int VW = (int)sizeof(V) / 4;
+        if (g == 0) {
+            vlo = reinterpret_cast<uintptr_t>(col + base);
+            vhi = reinterpret_cast<uintptr_t>(col + base + (long long)nnz);
+        } else if (g == 1) {
+            vlo = reinterpret_cast<uintptr_t>(val + base);
+            vhi = vlo + (uintptr_t)nnz * VW * 4;
+        } else {
+            vlo = reinterpret_cast<uintptr_t>(rp);
+            vhi = reinterpret_cast<uintptr_t>(rp + (long long)m + 1);
+        }
+    };
+    // Whether range g of block d, widened outwards to 16-byte boundaries,
+    // stays inside the view: then one bulk copy brings all of it (true for
+    // every block but those at the ends of the matrix).
+    auto widens = [&](const Range &r, const Span &sp, int g) {
+        uintptr_t vlo, vhi;
+        view_of(g, vlo, vhi);
+        const uintptr_t last = sp.first + (uintptr_t)r.n * 4;
+        return (sp.first & ~(uintptr_t)15) >= vlo && ((last + 15) & ~(uintptr_t)15) <= vhi;
+    };
+    // Lanes 0-2 each bulk-copy one range of block d into slot sl (widened to
+    // 16-byte boundaries where it may be, else its aligned middle); lane 0
+    // first arms the barrier with their total.  Called by the whole warp.
     auto issue = [&](int4 d, int sl) {
         const uint32_t bar = bar_base + 8 * sl;
         unsigned char *dst = wbuf + sl * S::BYTES;
-        const Span c = span_of(col, d.z, d.w, 4);
-        const Span v = span_of(val, d.z, d.w, (int)sizeof(V));
-        Span r{0, 0, 0};
-        if (d.y > 0) r = span_of(rp, d.x, (long long)d.x + d.y + 1, 4);
+        Range r{nullptr, 0, 0, 0};
+        uintptr_t lo = 0;
         uint32_t bytes = 0;
-        if (c.hi > c.lo) bytes += (uint32_t)(c.hi - c.lo);
-        if (v.hi > v.lo) bytes += (uint32_t)(v.hi - v.lo);
-        if (r.hi > r.lo) bytes += (uint32_t)(r.hi - r.lo);
-        mbar_expect_tx(bar, bytes);
-        if (c.hi > c.lo)
-            bulk_g2s(smem_u32(dst + S::C_OFF + (c.lo - (c.first & ~(uintptr_t)15))),
-                     reinterpret_cast<const void *>(c.lo), (uint32_t)(c.hi - c.lo), bar, pol);
-        if (v.hi > v.lo)
-            bulk_g2s(smem_u32(dst + S::V_OFF + (v.lo - (v.first & ~(uintptr_t)15))),
-                     reinterpret_cast<const void *>(v.lo), (uint32_t)(v.hi - v.lo), bar, pol);
-        if (r.hi > r.lo)
-            bulk_g2s(smem_u32(dst + S::R_OFF + (r.lo - (r.first & ~(uintptr_t)15))),
-                     reinterpret_cast<const void *>(r.lo), (uint32_t)(r.hi - r.lo), bar, 0);
-    };
-    // Lanes 0-23: the elements of block d outside the aligned middles (the
-    // ragged ends), by plain loads into slot sl.  Eight lanes per array:
-    // lanes 0-3 of a group take the head (at most 3 elements), lanes 4-7 the
-    // tail; a range with no aligned middle (at most 7 elements) is loaded by
-    // all eight.  Returns the element (index from k0) a lane loads, or -1.
-    auto edge = [&](const void *a, long long k0, long long n, int e, int l) -> long long {
-        const Span sp = span_of(a, k0, k0 + n, e);
-        long long k = l;
-        if (sp.hi > sp.lo) {
-            const long long head = (long long)((sp.lo - sp.first) / e);
-            const long long tail0 = (long long)((sp.hi - sp.first) / e);
-            if (l >= 4) k = tail0 + (l - 4);
-            else if (k >= head) return -1;
+        if (lane < 3) {
+            r = range_of(d, lane);
+            Span sp = span_of(r.a, r.k0, r.k0 + r.n, 4);
+            if (r.n > 0 && widens(r, sp, lane)) {
+                sp.lo = sp.first & ~(uintptr_t)15;
+                sp.hi = (sp.first + (uintptr_t)r.n * 4 + 15) & ~(uintptr_t)15;
+            }
+            if (r.n > 0 && sp.hi > sp.lo) {
+                bytes = (uint32_t)(sp.hi - sp.lo);
+                lo = sp.lo;
+            }
+            r.off += (uint32_t)(sp.lo - (sp.first & ~(uintptr_t)15));
         }
-        return k < n ? k : -1;
+        const uint32_t total = __shfl_sync(0xffffffffu, bytes, 0) +
+                               __shfl_sync(0xffffffffu, bytes, 1) +
+                               __shfl_sync(0xffffffffu, bytes, 2);
+        if (lane == 0) mbar_expect_tx(bar, total);
+        __syncwarp();  // armed before any copy can complete
+        if (bytes)
+            bulk_g2s(smem_u32(dst + r.off), reinterpret_cast<const void *>(lo), bytes, bar,
+                     lane == 2 ? 0 : pol);
     };
+    // Whether block d has a range that could not be widened (its ragged
+    // ends then come by plain loads); uniform over the warp.
+    auto needs_ragged = [&](int4 d) {
+        bool need = false;
+        if (lane < 3) {
+            const Range r = range_of(d, lane);
+            need = r.n > 0 && !widens(r, span_of(r.a, r.k0, r.k0 + r.n, 4), lane);
+        }
+        return __any_sync(0xffffffffu, need);
+    };
+    // Lanes 0-23: the words of block d outside the aligned middles (the
+    // ragged ends), by plain loads into slot sl; eight lanes per range.
+    // Lanes 0-3 of a group take the head (at most 3 words), lanes 4-7 the
+    // tail; a range with no aligned middle (at most 7 words) is loaded by all
+    // eight.
     auto ragged = [&](int4 d, int sl) {
-        unsigned char *dst = wbuf + sl * S::BYTES;
-        const int l = lane & 7;
-        if (lane < 8) {
-            const long long k = edge(col, d.z, (long long)d.w - d.z, 4, l);
-            if (k >= 0)
-                reinterpret_cast<int *>(dst + S::C_OFF)[(reinterpret_cast<uintptr_t>(col + d.z) & 15) / 4 + k] =
-                    __ldg(col + d.z + k);
-        } else if (lane < 16) {
-            const long long k = edge(val, d.z, (long long)d.w - d.z, (int)sizeof(V), l);
-            if (k >= 0)
-                reinterpret_cast<V *>(dst + S::V_OFF)[(reinterpret_cast<uintptr_t>(val + d.z) & 15) / sizeof(V) + k] =
-                    ld_stream(val + d.z + k);
-        } else if (lane < 24 && d.y > 0) {
-            const long long k = edge(rp, d.x, (long long)d.y + 1, 4, l);
-            if (k >= 0)
-                reinterpret_cast<int *>(dst + S::R_OFF)[(reinterpret_cast<uintptr_t>(rp + d.x) & 15) / 4 + k] =
-                    __ldg(rp + d.x + k);
+        const int g = lane >> 3, l = lane & 7;
+        if (g < 3) {
+            const Range r = range_of(d, g);
+            const Span sp = span_of(r.a, r.k0, r.k0 + r.n, 4);
+            if (r.n > 0 && widens(r, sp, g)) return;  // the bulk copy brings all of it
+            long long k = l;
+            if (sp.hi > sp.lo) {
+                const long long head = (long long)((sp.lo - sp.first) / 4);
+                const long long tail0 = (long long)((sp.hi - sp.first) / 4);
+                k = l >= 4 ? tail0 + (l - 4) : (l < head ? l : r.n);
+            }
+            if (k < r.n)
+                reinterpret_cast<unsigned *>(wbuf + sl * S::BYTES + r.off)[(sp.first & 15) / 4 + k] =
+                    __ldg(r.a + r.k0 + k);
         }
     };
 
+    pol = evict_first_policy();
     if (lane == 0) {
-        pol = evict_first_policy();
         for (int sl = 0; sl < kNbuf; ++sl) mbar_init(bar_base + 8 * sl, 1);
         mbar_fence_init();
-        for (int sl = 0; sl < kNbuf; ++sl)
-            if (b + sl * W < nblk) issue(__ldg(desc + b + sl * W), sl);
     }
     __syncwarp();
+    for (int sl = 0; sl < kNbuf; ++sl)
+        if (b + sl * W < nblk) issue(__ldg(desc + b + sl * W), sl);
 
     int polls = first_wait >= 0 && blockIdx.x == 0 && warp == 0 ? first_wait : kWaitPolls;
     uint32_t phases = 0u;
@@ -184,11 +232,11 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
     for (; b < nblk; b += W) {
         double yv = 0.0;
         if (beta != 0.0 && lane < d.y) yv = ld_y(y + d.x + lane, streaming);
-        ragged(d, sl);
+        if (needs_ragged(d)) ragged(d, sl);
         int4 dn = make_int4(0, 0, 0, 0), df = make_int4(0, 0, 0, 0);
         if (b + W < nblk) dn = __ldg(desc + b + W);
         const bool more = b + kNbuf * W < nblk;
-        if (lane == 0 && more) df = __ldg(desc + b + kNbuf * W);
+        if (more) df = __ldg(desc + b + kNbuf * W);
         if (!mbar_wait(bar_base + 8 * sl, (phases >> sl) & 1u, polls)) {
             timeout = 1;
             break;
@@ -204,29 +252,25 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
                       (int)((reinterpret_cast<uintptr_t>(val + d.z) & 15) / sizeof(V));
         double *Ps = sizeof(V) == 8 ? reinterpret_cast<double *>(const_cast<V *>(Vs))
                                     : reinterpret_cast<double *>(sb + S::P_OFF);
-        // 1. products in nnz order, 4 loads of a lane in flight together
-        constexpr int U = 4;
-        for (int base = 0; base < nz; base += 32 * U) {
-            int c[U];
-            V v[U], xv[U];
+        // 1. products in nnz order: every x gather of the lane (up to
+        // kRowsNmax / 32) is issued before any product is formed
+        constexpr int UM = kRowsNmax / 32;
+        int c[UM];
+        V xv[UM];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int i = base + u * 32 + lane;
-                if (i < nz) {
-                    c[u] = Cs[i];
-                    v[u] = Vs[i];
-                }
-            }
+        for (int u = 0; u < UM; ++u) {
+            const int i = u * 32 + lane;
+            if (i < nz) c[u] = Cs[i];
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int i = base + u * 32 + lane;
-                if (i < nz) xv[u] = ld_keep(x + c[u], keep);
-            }
+        for (int u = 0; u < UM; ++u) {
+            const int i = u * 32 + lane;
+            if (i < nz) xv[u] = ld_keep(x + c[u], keep);
+        }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int i = base + u * 32 + lane;
-                if (i < nz) Ps[i] = PT::make(v[u], xv[u]);
-            }
+        for (int u = 0; u < UM; ++u) {
+            const int i = u * 32 + lane;
+            if (i < nz) Ps[i] = PT::make(Vs[i], xv[u]);
         }
         __syncwarp();
         // 2. rows (lane i: row d.x + i) or the piece of a long row
@@ -266,7 +310,7 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
         // ordered before the bulk copies that refill it
         fence_proxy_async();
         __syncwarp();
-        if (lane == 0 && more) issue(df, sl);
+        if (more) issue(df, sl);
         sl = sl + 1 == kNbuf ? 0 : sl + 1;
         d = dn;
     }
@@ -381,7 +425,8 @@ void launch_rows_t(const RowsPlan &R, const Plan *p, double alpha, const typenam
     hook_start(s);
     kern<<<grid, RW * 32, smem, s>>>(R.nblk, R.desc, p->rowptr, p->col,
                                      static_cast<const V *>(p->val), x, y, alpha, beta,
-                                     R.carry_val, p->status, first_wait_budget());
+                                     R.carry_val, p->status, first_wait_budget(), p->m,
+                                     p->base, p->nnz);
     hook_stop(s);
     launch_fixup(p->m, R.carry_row, R.carry_val, R.nblk, R.runs, alpha, y, nullptr, s);
 }

@@ -195,15 +195,19 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
     }
 
     // 4. warp segmented scan of lane carries, reset at lanes that start a row
+    // A lane adds the partial scan from o lanes back while no row starts in
+    // the o lanes ending at it: o <= d, d = distance to the last lane at or
+    // before it that starts a row (its own index when none does).  These are
+    // exactly the additions of the flag-carrying segmented scan, in the same
+    // order, without shuffling the flags.
     double cv = acc.get();  // tail (or whole lane when no row starts here)
-    unsigned f = started;
+    {
+        const unsigned below = __ballot_sync(0xffffffffu, started) & (0xffffffffu >> (31 - lane));
+        const int d = below ? lane - (31 - __clz(below)) : lane;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        double vu = __shfl_up_sync(0xffffffffu, cv, o);
-        unsigned fu = __shfl_up_sync(0xffffffffu, f, o);
-        if (lane >= o) {
-            if (!f) cv += vu;
-            f |= fu;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double vu = __shfl_up_sync(0xffffffffu, cv, o);
+            if (o <= d) cv += vu;
         }
     }
     double incoming = __shfl_up_sync(0xffffffffu, cv, 1);
