@@ -32,7 +32,6 @@ constexpr int BW = BT / 32;
 constexpr int SEG = 32 * kBatchIpt;
 constexpr uint32_t TBB = (uint32_t)tile_bytes_of(kBatchSigma, 8);
 constexpr int TG = kBatchTileGroup;
-constexpr uint32_t kBit0 = 32 * kBatchSigma * 12;  // offset of a tile's row-start bits
 static_assert(TBB % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // Per class kernel: dynamic shared memory per warp (merge: a segment's
@@ -188,14 +187,6 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
                 }
                 const int t0 = local * TG;
                 const int nt = M.tiles - t0 < TG ? M.tiles - t0 : TG;
-                // tile_seg of the unit's tiles (lane j: tile t0+j) and the
-                // row-start bit of the tile after the unit
-                const int tseg_l = lane < nt ? __ldg(M.tile_seg + t0 + lane) : 0;
-                const unsigned nb_last =
-                    t0 + nt < M.tiles
-                        ? (__ldg(reinterpret_cast<const unsigned *>(
-                               M.blob + (size_t)(t0 + nt) * TBB + kBit0)) & 1u)
-                        : 0u;
                 if (!mbar_wait(bar0 + 8 * cur, (phases >> cur) & 1u)) {
                     // let the copies still in flight land (bounded) before the
                     // warp leaves: this unit's and, if started, the next one's
@@ -213,17 +204,12 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
                 for (int j = 0; j < nt; ++j) {
                     const int t = t0 + j;
                     const unsigned char *tj = tb + j * TBB;
-                    unsigned nb0 = nb_last;
-                    if (j + 1 < nt) {  // the next tile's x, in flight during this reduce
-                        nb0 = *reinterpret_cast<const unsigned *>(tj + TBB + kBit0) & 1u;
+                    if (j + 1 < nt)  // the next tile's x, in flight during this reduce
                         tile_gather<ProdF64, kBatchSigma>(t + 1, M.tiles, M.nnz, tj + TBB, M.x,
                                                           keep, xn);
-                    }
-                    const int tseg = __shfl_sync(0xffffffffu, tseg_l, j);
-                    tile_reduce<ProdF64, AccF64, kBatchSigma>(t, t == M.tiles - 1, tj, tseg, nb0,
-                                                              M.ne, xv, M.y, M.alpha, M.beta,
-                                                              M.carry_val, streaming, 0.0, 0.0,
-                                                              nullptr);
+                    tile_reduce<ProdF64, AccF64, kBatchSigma>(t, tj, M.ne, xv, M.y, M.alpha,
+                                                              M.beta, M.carry_val, streaming, 0.0,
+                                                              0.0, nullptr);
 #pragma unroll
                     for (int q = 0; q < kBatchSigma; ++q) xv[q] = xn[q];
                 }

@@ -3,8 +3,8 @@
 // A kernel of its own beside the three that replace the reference's
 // cusparseDcsrmv / cusparseDcsrmv_mp / CSR5 calls (SparseBLAS/src/
 // dspmv_mgpu_v1.cu:195-217): the rows are cut into blocks of at most 32
-// consecutive rows and at most kRowsNmax nnz, and a row longer than kRowsNmax
-// into pieces of kRowsNmax nnz (the row-blocking idea of CSR-Adaptive,
+// consecutive rows and at most NMAX nnz (256 or 384, per plan), and a row
+// longer than NMAX into pieces of NMAX nnz (the row-blocking idea of CSR-Adaptive,
 // Greathouse & Daga, SC'14).  The blocks are fixed per plan and use the
 // caller's CSR arrays as they are: there is no copy of the matrix.
 //
@@ -29,6 +29,7 @@
 // copies of a warp's next block are in flight while it reduces the current
 // one.
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <cub/cub.cuh>
 
@@ -42,19 +43,25 @@ namespace sbb {
 namespace {
 
 constexpr int RW = 4;              // warps per CTA
-constexpr int kRowsNmax = 384;     // nnz per block (and per piece of a long row)
+// Block shapes (nnz per block and per piece of a long row; CTAs per SM the
+// launch bounds aim at): a plan picks one when it is built.
+struct RowsShape {
+    int nmax, minb;
+};
+constexpr RowsShape kRowsShapes[] = {{256, 8}, {384, 5}};
+constexpr int kRowsDefaultShape = 1;
 constexpr int kRowsPerBlock = 32;  // rows per block (one per lane)
-constexpr int kWarpRow = 32;       // rows of a block longer than this: summed by the warp
+constexpr int kWarpRow = 16;       // rows of a block longer than this: summed by the warp
 constexpr int kNbuf = 2;           // blocks in shared memory per warp
 
 // Shared-memory slot of one block.  Element k of a range sits at
 // (its byte address mod 16) / size + (k - first), so the 16-byte-aligned
 // middle of the range lands on a 16-byte boundary for the bulk copy.
-template <typename V> struct RowsSlot {
-    static constexpr int CI = kRowsNmax + 4;                         // columns (int)
-    static constexpr int VN = kRowsNmax + 16 / (int)sizeof(V);       // values (V)
+template <typename V, int NMAX> struct RowsSlot {
+    static constexpr int CI = NMAX + 4;                              // columns (int)
+    static constexpr int VN = NMAX + 16 / (int)sizeof(V);            // values (V)
     static constexpr int RI = kRowsPerBlock + 1 + 3 + 4;             // row pointers (int)
-    static constexpr int PN = sizeof(V) == 8 ? 0 : kRowsNmax;        // FP32: products (double)
+    static constexpr int PN = sizeof(V) == 8 ? 0 : NMAX;             // FP32: products (double)
     static constexpr uint32_t C_OFF = 0;
     static constexpr uint32_t V_OFF = C_OFF + CI * 4;
     static constexpr uint32_t R_OFF = V_OFF + ((VN * (int)sizeof(V) + 15) / 16) * 16;
@@ -84,8 +91,8 @@ __device__ __forceinline__ Span span_of(const void *a, long long k0, long long k
 // Block descriptor: x = first row, y = rows (>= 1), or 0 for the last piece
 // of a long row (it writes y), or -1 for another piece (it leaves a carry);
 // z, w = nnz range [k0, k1) (absolute offsets, as the row pointer holds them).
-template <typename PT>
-__global__ void __launch_bounds__(RW * 32, 5)
+template <typename PT, int NMAX, int MINB>
+__global__ void __launch_bounds__(RW * 32, MINB)
 rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
             const int *__restrict__ col, const typename PT::V *__restrict__ val,
             const typename PT::V *__restrict__ x, double *__restrict__ y, double alpha,
@@ -93,7 +100,7 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
             int m, int base, int nnz)
 {
     using V = typename PT::V;
-    using S = RowsSlot<V>;
+    using S = RowsSlot<V, NMAX>;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[RW][kNbuf];
     // columns were range-checked when the plan was built; a failed check
@@ -253,8 +260,8 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
         double *Ps = sizeof(V) == 8 ? reinterpret_cast<double *>(const_cast<V *>(Vs))
                                     : reinterpret_cast<double *>(sb + S::P_OFF);
         // 1. products in nnz order: every x gather of the lane (up to
-        // kRowsNmax / 32) is issued before any product is formed
-        constexpr int UM = kRowsNmax / 32;
+        // NMAX / 32) is issued before any product is formed
+        constexpr int UM = NMAX / 32;
         int c[UM];
         V xv[UM];
 #pragma unroll
@@ -328,11 +335,12 @@ rows_kernel(int nblk, const int4 *__restrict__ desc, const int *__restrict__ rp,
 // ---- plan: the block list ---------------------------------------------------
 // Rows are taken in groups of 32 (so blocks never straddle a group and the y
 // stores of a block stay within one 256-byte row group); inside a group, rows
-// are packed greedily into blocks of at most kRowsNmax nnz, and a row with
-// more than kRowsNmax nnz becomes its own run of pieces.  One thread per
+// are packed greedily into blocks of at most nmax nnz, and a row with
+// more than nmax nnz becomes its own run of pieces.  One thread per
 // group counts its blocks, a scan places them, a second pass writes them.
 template <bool EMIT>
-__global__ void rows_blocks_kernel(const int *__restrict__ rp, int m, int *__restrict__ count,
+__global__ void rows_blocks_kernel(const int *__restrict__ rp, int m, int nmax,
+                                   int *__restrict__ count,
                                    const int *__restrict__ offset, int4 *__restrict__ desc,
                                    int *__restrict__ carry_row)
 {
@@ -353,10 +361,10 @@ __global__ void rows_blocks_kernel(const int *__restrict__ rp, int m, int *__res
     int lo = rp[r0];
     for (int r = r0; r < r1; ++r) {
         const int hi = rp[r + 1], len = hi - lo;
-        if (len > kRowsNmax) {
+        if (len > nmax) {
             if (rows) close(r);
-            for (long long k = lo; k < hi; k += kRowsNmax) {
-                const long long k1 = min((long long)hi, k + kRowsNmax);
+            for (long long k = lo; k < hi; k += nmax) {
+                const long long k1 = min((long long)hi, k + nmax);
                 if (EMIT) {
                     desc[out] = make_int4(r, k1 == hi ? 0 : -1, (int)k, (int)k1);
                     carry_row[out] = k1 == hi ? m : r;
@@ -366,7 +374,7 @@ __global__ void rows_blocks_kernel(const int *__restrict__ rp, int m, int *__res
             start = r + 1;
             rows = nz = 0;
         } else {
-            if (rows && nz + len > kRowsNmax) {
+            if (rows && nz + len > nmax) {
                 close(r);
                 start = r;
                 rows = nz = 0;
@@ -392,6 +400,7 @@ __global__ void rows_col_check_kernel(const int *__restrict__ col, long long fir
 }
 
 struct RowsPlan {
+    int shape = kRowsDefaultShape;  // index into kRowsShapes
     int nblk = 0;
     int4 *desc = nullptr;
     int *carry_row = nullptr;
@@ -407,13 +416,13 @@ int grid_of(long long work, int tpb)
     return (int)g;
 }
 
-template <typename PT>
-void launch_rows_t(const RowsPlan &R, const Plan *p, double alpha, const typename PT::V *x,
+template <typename PT, int NMAX, int MINB>
+void launch_rows_n(const RowsPlan &R, const Plan *p, double alpha, const typename PT::V *x,
                    double beta, double *y, cudaStream_t s)
 {
     using V = typename PT::V;
-    auto kern = rows_kernel<PT>;
-    constexpr size_t smem = (size_t)RW * kNbuf * RowsSlot<V>::BYTES;
+    auto kern = rows_kernel<PT, NMAX, MINB>;
+    constexpr size_t smem = (size_t)RW * kNbuf * RowsSlot<V, NMAX>::BYTES;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, sms = 148, occ = 1;
     cudaGetDevice(&dev);
@@ -428,6 +437,17 @@ void launch_rows_t(const RowsPlan &R, const Plan *p, double alpha, const typenam
                                      R.carry_val, p->status, first_wait_budget(), p->m,
                                      p->base, p->nnz);
     hook_stop(s);
+}
+
+template <typename PT>
+void launch_rows_t(const RowsPlan &R, const Plan *p, double alpha, const typename PT::V *x,
+                   double beta, double *y, cudaStream_t s)
+{
+    static_assert(sizeof(kRowsShapes) / sizeof(kRowsShapes[0]) == 2, "one launch per shape");
+    if (R.shape == 0)
+        launch_rows_n<PT, kRowsShapes[0].nmax, kRowsShapes[0].minb>(R, p, alpha, x, beta, y, s);
+    else
+        launch_rows_n<PT, kRowsShapes[1].nmax, kRowsShapes[1].minb>(R, p, alpha, x, beta, y, s);
     launch_fixup(p->m, R.carry_row, R.carry_val, R.nblk, R.runs, alpha, y, nullptr, s);
 }
 
@@ -437,6 +457,11 @@ int rows_build(Plan *p, cudaStream_t s)
 {
     auto *R = new RowsPlan();
     p->rows = R;
+    // SBB_ROWS_SHAPE (0 or 1) overrides the default block shape
+    if (const char *e = getenv("SBB_ROWS_SHAPE")) {
+        const int v = atoi(e);
+        if (v == 0 || v == 1) R->shape = v;
+    }
     const int m = p->m;
     const long long groups = ((long long)m + kRowsPerBlock - 1) / kRowsPerBlock;
     auto al = [&](void **ptr, size_t bytes) {
@@ -457,7 +482,7 @@ int rows_build(Plan *p, cudaStream_t s)
     SBB_CUDA(cudaMemsetAsync(count + groups, 0, sizeof(int), s));
     if (groups > 0)
         rows_blocks_kernel<false><<<(int)((groups + 255) / 256), 256, 0, s>>>(
-            p->rowptr, m, count, nullptr, nullptr, nullptr);
+            p->rowptr, m, kRowsShapes[R->shape].nmax, count, nullptr, nullptr, nullptr);
     size_t tmp_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, count, offset, groups + 1, s);
     void *tmp = nullptr;
@@ -478,7 +503,7 @@ int rows_build(Plan *p, cudaStream_t s)
     }
     if (groups > 0)
         rows_blocks_kernel<true><<<(int)((groups + 255) / 256), 256, 0, s>>>(
-            p->rowptr, m, nullptr, offset, R->desc, R->carry_row);
+            p->rowptr, m, kRowsShapes[R->shape].nmax, nullptr, offset, R->desc, R->carry_row);
     if (nblk > 0) {
         int rc = carry_runs_build(R->carry_row, nblk, m, &R->runs, s);
         if (rc) return rc;

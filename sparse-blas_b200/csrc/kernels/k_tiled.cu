@@ -9,12 +9,16 @@
 //     to a power of two in {4, 8, 16, 32}.
 //   * The plan keeps a COPY of the matrix as one blob per tile (the reference
 //     transposes the caller's arrays in place, format_cuda.h:525-744):
-//         [int cols[TILE] | V vals[TILE] | uint32 row-start bitmap[sigma]]
+//         [int cols[TILE] | V vals[TILE] | uint32 row-start bitmap[sigma] |
+//          header: segment rank, closing / row-start flags, per-lane counts
+//          of earlier row starts]
 //     Inside a tile, nnz go in groups of 4 per lane, laid out so every
 //     shared-memory read is 16 contiguous bytes per lane (no bank conflicts).
 //   * One bit per nnz marks row starts (CSR5's bit-flag descriptor,
-//     format_cuda.h:129-360, without the packed y/scan offsets: the row of
-//     each segment comes from a warp scan of the lanes' popcounts).
+//     format_cuda.h:129-360).  The header plays the part of CSR5's tile
+//     pointer and per-lane y offsets (format_cuda.h:362-523) in a layout of
+//     its own: it arrives with the tile's bulk copy, so a tile needs no
+//     metadata loads and no prefix scan of row starts.
 //   * Persistent warps take tiles round-robin.  Each warp double-buffers tiles
 //     in shared memory with one TMA bulk copy per tile (cp.async.bulk +
 //     mbarrier, evict-first so x stays in L2; every wait is bounded).  All x
@@ -153,6 +157,38 @@ __global__ void tile_seg_kernel(const int *__restrict__ rp, int m, int sigma, in
     tile_seg[t] = rank ? rank[lo] : lo;
 }
 
+// Tile headers (tiled_device.cuh): segment rank, closing and row-start
+// flags, and each lane's count of earlier row starts.  One thread per tile.
+__global__ void tile_header_kernel(const int *__restrict__ tile_seg, int sigma, int vbytes,
+                                   int tiles, unsigned char *__restrict__ blob)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tiles) return;
+    const long long TILE = 32LL * sigma;
+    const size_t TB = tile_bytes_of(sigma, vbytes);
+    unsigned char *tb = blob + (size_t)t * TB;
+    const unsigned *bits = reinterpret_cast<const unsigned *>(tb + TILE * (4 + vbytes));
+    unsigned char *hdr = tb + tile_hdr_offset(sigma, vbytes);
+    const unsigned next0 =
+        t + 1 < tiles ? *reinterpret_cast<const unsigned *>(blob + (size_t)(t + 1) * TB +
+                                                            TILE * (4 + vbytes)) & 1u
+                      : 1u;  // the last tile closes its open row
+    reinterpret_cast<int *>(hdr)[0] = tile_seg[t];
+    reinterpret_cast<int *>(hdr)[1] =
+        (int)((next0 ? kTileCloses : 0u) | ((bits[0] & 1u) ? kTileStartsRow : 0u));
+    int acc = 0;
+    for (int l = 0; l < 32; ++l) {
+        if (sigma <= 8)
+            hdr[16 + l] = (unsigned char)acc;
+        else
+            reinterpret_cast<unsigned short *>(hdr + 16)[l] = (unsigned short)acc;
+        const unsigned lb = sigma == 32 ? bits[l]
+                                        : (bits[(l * sigma) >> 5] >> ((l * sigma) & 31)) &
+                                              ((1u << sigma) - 1u);
+        acc += __popc(lb);
+    }
+}
+
 __device__ __forceinline__ unsigned first_bit_of_tile(const unsigned char *blob, size_t TB,
                                                       long long TILE, int vbytes, int t)
 {
@@ -204,7 +240,6 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
              int first_wait)
 {
     using V = typename PT::V;
-    constexpr int TILE = 32 * SIGMA;
     constexpr uint32_t TB = (uint32_t)tile_bytes_of(SIGMA, sizeof(V));
     constexpr uint32_t SB = (uint32_t)sum_bytes_of(SIGMA);
     extern __shared__ __align__(128) unsigned char smem[];
@@ -235,11 +270,6 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
     }
     __syncwarp();
 
-    auto next_bit0_of = [&](int tt) -> unsigned {
-        return tt + 1 < tiles ? (__ldg(reinterpret_cast<const unsigned *>(
-                                     blob + (size_t)(tt + 1) * TB + TILE * (4 + sizeof(V)))) & 1u)
-                              : 0u;
-    };
     unsigned timeout = 0;
     uint32_t phases = 0u;  // bit b: parity of buffer b's next phase
     const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
@@ -253,31 +283,29 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
         return ok;
     };
     int b = 0;
+    // Tiles of sigma >= 8 load y of the segments they can write before the
+    // tile arrives, from the segment ranks of this tile and the next one.
     int tseg = 0, tseg1 = 0;
-    unsigned nb0 = 0;
-    if (t < tiles) {
+    if (SIGMA >= 8 && t < tiles) {
         tseg = __ldg(tile_seg + t);
         tseg1 = __ldg(tile_seg + t + 1);
-        nb0 = next_bit0_of(t);
     }
     for (; t < tiles; t += W) {
-        // y of the segments this tile can write (tile_seg[t] .. tile_seg[t+1]),
-        // loaded now so the write pass does not wait for it
         double ya = 0.0, yb = 0.0;
-        if (SIGMA >= 8 && beta != 0.0) {
-            const int lim = tseg1 + (t + 1 < tiles ? 1 : 0);
-            if (tseg + lane < lim) ya = ld_y(y + (ne ? __ldg(ne + tseg + lane) : tseg + lane), streaming);
-            if (tseg + 32 + lane < lim)
-                yb = ld_y(y + (ne ? __ldg(ne + tseg + 32 + lane) : tseg + 32 + lane), streaming);
-        }
-        // metadata of the next tile, in flight while this one is reduced
-        const int tn = t + W;
         int tseg_n = 0, tseg1_n = 0;
-        unsigned nb0_n = 0;
-        if (tn < tiles) {
-            tseg_n = __ldg(tile_seg + tn);
-            tseg1_n = __ldg(tile_seg + tn + 1);
-            nb0_n = next_bit0_of(tn);
+        if (SIGMA >= 8) {
+            if (beta != 0.0) {
+                const int lim = tseg1 + (t + 1 < tiles ? 1 : 0);
+                if (tseg + lane < lim)
+                    ya = ld_y(y + (ne ? __ldg(ne + tseg + lane) : tseg + lane), streaming);
+                if (tseg + 32 + lane < lim)
+                    yb = ld_y(y + (ne ? __ldg(ne + tseg + 32 + lane) : tseg + 32 + lane), streaming);
+            }
+            const int tn = t + W;  // segment ranks of the next tile, in flight meanwhile
+            if (tn < tiles) {
+                tseg_n = __ldg(tile_seg + tn);
+                tseg1_n = __ldg(tile_seg + tn + 1);
+            }
         }
         if (!wait_buf(b)) {
             timeout = 1;
@@ -285,14 +313,13 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
         }
         V xv[SIGMA];
         tile_gather<PT, SIGMA>(t, tiles, nnz, wbuf + b * TB, x, keep, xv);
-        tile_reduce<PT, ACC, SIGMA>(t, t == tiles - 1, wbuf + b * TB, tseg, nb0, ne, xv, y, alpha,
-                                    beta, carry_val, streaming, ya, yb, s_sum);
+        tile_reduce<PT, ACC, SIGMA>(t, wbuf + b * TB, ne, xv, y, alpha, beta, carry_val, streaming,
+                                    ya, yb, s_sum);
         __syncwarp();  // every lane is done with buffer b before it is refilled
         if (lane == 0 && t + NBUF * W < tiles) issue(t + NBUF * W, b);
         b = b + 1 == NBUF ? 0 : b + 1;
         tseg = tseg_n;
         tseg1 = tseg1_n;
-        nb0 = nb0_n;
     }
     if (timeout) {
         // Let every copy still in flight land (bounded) before the warp
@@ -481,6 +508,8 @@ int tiled_build(Plan *p, cudaStream_t s)
             T->tile_seg);
         carry_rows_kernel<<<(T->tiles + 255) / 256, 256, 0, s>>>(
             T->blob, T->sigma, vbytes, T->tile_seg, T->ne, T->tiles, m, T->carry_row);
+        tile_header_kernel<<<(T->tiles + 255) / 256, 256, 0, s>>>(T->tile_seg, T->sigma, vbytes,
+                                                                  T->tiles, T->blob);
         int rc = carry_runs_build(T->carry_row, T->tiles, m, &T->runs, s);
         if (rc) return rc;
         p->scratch_bytes += T->runs.bytes;

@@ -9,10 +9,30 @@
 
 namespace sbb {
 
-__host__ __device__ constexpr size_t tile_bytes_of(int sigma, int vbytes)
+// A tile blob:
+//   [int cols[TILE] | V vals[TILE] | uint32 row-start bits[sigma] | header]
+// The header holds what the reduction of a tile needs beyond its nnz, so it
+// arrives with the same bulk copy instead of costing loads and scans:
+//   int seg    segment rank (row, when no row is empty) of the row holding
+//              the tile's first nnz;
+//   int flags  bit 0: the row open at the tile's end closes in it (the next
+//              tile starts a row, or this is the last tile); bit 1: the
+//              tile's first nnz starts a row;
+//   8 bytes of padding, then per lane the number of row starts in the lanes
+//   before it (uint8 for sigma <= 8, uint16 above).
+__host__ __device__ constexpr size_t tile_hdr_offset(int sigma, int vbytes)
 {
     return (size_t)32 * sigma * (4 + vbytes) + 4 * (size_t)sigma;
 }
+__host__ __device__ constexpr size_t tile_hdr_bytes(int sigma)
+{
+    return 16 + 32 * (sigma <= 8 ? 1 : 2);
+}
+__host__ __device__ constexpr size_t tile_bytes_of(int sigma, int vbytes)
+{
+    return tile_hdr_offset(sigma, vbytes) + tile_hdr_bytes(sigma);
+}
+constexpr unsigned kTileCloses = 1u, kTileStartsRow = 2u;
 // Per-warp staging of a tile's row sums: up to 32*sigma + 1 segments (only
 // tiles of sigma >= 8 stage them).
 __host__ __device__ constexpr size_t sum_bytes_of(int sigma)
@@ -111,15 +131,16 @@ __device__ __forceinline__ void tile_gather(int t, int tiles, long long nnz, con
     }
 }
 
-// Reduces one tile whose x values are already gathered (xv).  Tiles of
-// sigma >= 8 stage row sums in the warp's s_sum (index = segment - tseg) and
-// write them to y in one coalesced pass at the end, so the divergent per-nnz
-// loop touches no global memory; ya/yb hold y of segments tseg+lane and
-// tseg+32+lane, loaded when the tile started.  Tiles of sigma < 8 write each
-// row as it completes.
+// Reduces one tile whose x values are already gathered (xv).  The tile's
+// segment rank, closing flag and each lane's count of earlier row starts come
+// from its header.  Tiles of sigma >= 8 stage row sums in the warp's s_sum
+// (index = segment - tseg) and write them to y in one coalesced pass at the
+// end, so the divergent per-nnz loop touches no global memory; ya/yb hold y
+// of segments tseg+lane and tseg+32+lane, loaded when the tile started.
+// Tiles of sigma < 8 write each row as it completes.
 template <typename PT, typename ACC, int SIGMA>
-__device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned char *tb, int tseg,
-                                            unsigned next_bit0, const int *__restrict__ ne,
+__device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
+                                            const int *__restrict__ ne,
                                             const typename PT::V (&xv)[SIGMA],
                                             double *__restrict__ y, double alpha, double beta,
                                             double *__restrict__ carry_val, uint64_t stream,
@@ -128,16 +149,26 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
     using V = typename PT::V;
     constexpr int TILE = 32 * SIGMA;
     constexpr int G = SIGMA / 4;
+    constexpr size_t HDR = tile_hdr_offset(SIGMA, sizeof(V));
     const int lane = threadIdx.x & 31;
     const V *s_val = reinterpret_cast<const V *>(tb + TILE * 4);
     const unsigned *s_bits = reinterpret_cast<const unsigned *>(tb + TILE * (4 + sizeof(V)));
 
-    // this lane's sigma row-start bits
+    // this lane's sigma row-start bits and the tile's header
     unsigned bits;
     if constexpr (SIGMA == 32)
         bits = s_bits[lane];
     else
         bits = (s_bits[(lane * SIGMA) >> 5] >> ((lane * SIGMA) & 31)) & ((1u << SIGMA) - 1u);
+    const int2 hdr = *reinterpret_cast<const int2 *>(tb + HDR);
+    const int tseg = hdr.x;
+    const bool closes = hdr.y & kTileCloses;  // the row open at the end ends here
+    const unsigned b0 = (hdr.y & kTileStartsRow) ? 1u : 0u;
+    int excl;  // row starts in the lanes before this one
+    if constexpr (SIGMA <= 8)
+        excl = tb[HDR + 16 + lane];
+    else
+        excl = reinterpret_cast<const unsigned short *>(tb + HDR + 16)[lane];
 
     // 2. segment rows of this lane.  Tiles of sigma >= 8 stage row sums and
     // write them in one coalesced pass; sigma = 4 tiles (few rows per lane,
@@ -150,15 +181,7 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
             write_y(y + (ne ? __ldg(ne + sg) : sg), alpha, sum, beta, stream);
         }
     };
-    const unsigned b0 = __shfl_sync(0xffffffffu, bits, 0) & 1u;
-    const int cnt = __popc(bits);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int u = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += u;
-    }
-    const int head_seg = tseg - (int)b0 + incl - cnt;  // segment open before this lane's first nnz
+    const int head_seg = tseg - (int)b0 + excl;  // segment open before this lane's first nnz
 
     // 3. products and lane-local segmented sums
     ACC acc;
@@ -216,18 +239,15 @@ __device__ __forceinline__ void tile_reduce(int t, bool last, const unsigned cha
     // lane 0 with a start on its first nnz that row ended with the previous
     // tile, which wrote it.
     if (started && !(lane == 0 && b0)) put(head_seg, incoming + head);
-    const bool closes = last || next_bit0;  // the open row ends with this tile
     if (lane == 31) {
-        if (closes) {
-            put(seg, cv);
-            carry_val[t] = 0.0;  // carry_row[t] == m
-        } else {
+        if (closes)
+            put(seg, cv);        // carry_row[t] == m: no carry is read for this tile
+        else
             carry_val[t] = cv;   // carried into row_of(seg) == carry_row[t]
-        }
     }
     if (!kStaged) return;
     // 5. rows completed here: segments tseg .. tseg+nwrite-1, coalesced
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int total = __shfl_sync(0xffffffffu, excl + __popc(bits), 31);
     const int nwrite = total + (closes ? 1 : 0) - (int)b0;
     __syncwarp();
     for (int i = lane; i < nwrite; i += 32) {
