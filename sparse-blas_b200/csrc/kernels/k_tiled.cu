@@ -158,34 +158,40 @@ __global__ void tile_seg_kernel(const int *__restrict__ rp, int m, int sigma, in
 }
 
 // Tile headers (tiled_device.cuh): segment rank, closing and row-start
-// flags, and each lane's count of earlier row starts.  One thread per tile.
+// flags, and each lane's count of earlier row starts.  One warp per tile:
+// lane l counts its own row starts, a warp scan gives the offsets.
 __global__ void tile_header_kernel(const int *__restrict__ tile_seg, int sigma, int vbytes,
                                    int tiles, unsigned char *__restrict__ blob)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= tiles) return;
+    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= tiles) return;  // whole warps leave together
     const long long TILE = 32LL * sigma;
     const size_t TB = tile_bytes_of(sigma, vbytes);
     unsigned char *tb = blob + (size_t)t * TB;
     const unsigned *bits = reinterpret_cast<const unsigned *>(tb + TILE * (4 + vbytes));
     unsigned char *hdr = tb + tile_hdr_offset(sigma, vbytes);
-    const unsigned next0 =
-        t + 1 < tiles ? *reinterpret_cast<const unsigned *>(blob + (size_t)(t + 1) * TB +
-                                                            TILE * (4 + vbytes)) & 1u
-                      : 1u;  // the last tile closes its open row
-    reinterpret_cast<int *>(hdr)[0] = tile_seg[t];
-    reinterpret_cast<int *>(hdr)[1] =
-        (int)((next0 ? kTileCloses : 0u) | ((bits[0] & 1u) ? kTileStartsRow : 0u));
-    int acc = 0;
-    for (int l = 0; l < 32; ++l) {
-        if (sigma <= 8)
-            hdr[16 + l] = (unsigned char)acc;
-        else
-            reinterpret_cast<unsigned short *>(hdr + 16)[l] = (unsigned short)acc;
-        const unsigned lb = sigma == 32 ? bits[l]
-                                        : (bits[(l * sigma) >> 5] >> ((l * sigma) & 31)) &
-                                              ((1u << sigma) - 1u);
-        acc += __popc(lb);
+    const unsigned lb = sigma == 32 ? bits[lane]
+                                    : (bits[(lane * sigma) >> 5] >> ((lane * sigma) & 31)) &
+                                          ((1u << sigma) - 1u);
+    const int cnt = __popc(lb);
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (sigma <= 8)
+        hdr[16 + lane] = (unsigned char)(incl - cnt);
+    else
+        reinterpret_cast<unsigned short *>(hdr + 16)[lane] = (unsigned short)(incl - cnt);
+    if (lane == 0) {
+        const unsigned next0 =
+            t + 1 < tiles ? *reinterpret_cast<const unsigned *>(blob + (size_t)(t + 1) * TB +
+                                                                TILE * (4 + vbytes)) & 1u
+                          : 1u;  // the last tile closes its open row
+        reinterpret_cast<int *>(hdr)[0] = tile_seg[t];
+        reinterpret_cast<int *>(hdr)[1] =
+            (int)((next0 ? kTileCloses : 0u) | ((bits[0] & 1u) ? kTileStartsRow : 0u));
     }
 }
 
@@ -508,8 +514,8 @@ int tiled_build(Plan *p, cudaStream_t s)
             T->tile_seg);
         carry_rows_kernel<<<(T->tiles + 255) / 256, 256, 0, s>>>(
             T->blob, T->sigma, vbytes, T->tile_seg, T->ne, T->tiles, m, T->carry_row);
-        tile_header_kernel<<<(T->tiles + 255) / 256, 256, 0, s>>>(T->tile_seg, T->sigma, vbytes,
-                                                                  T->tiles, T->blob);
+        tile_header_kernel<<<(int)(((long long)T->tiles * 32 + 255) / 256), 256, 0, s>>>(
+            T->tile_seg, T->sigma, vbytes, T->tiles, T->blob);
         int rc = carry_runs_build(T->carry_row, T->tiles, m, &T->runs, s);
         if (rc) return rc;
         p->scratch_bytes += T->runs.bytes;
