@@ -395,10 +395,15 @@ def run_reference_batch(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local):
+def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local, kernel64=None,
+                kw64=None):
     """FP32-storage compensated form vs the FP64 plan on the same matrix, both
     timed here (main kernel with CUDA events, whole steps), with max and
-    median per-row error against the FP64 double-double oracle."""
+    median per-row error against the FP64 double-double oracle.  kernel / kw
+    configure the FP32 plan, kernel64 / kw64 the FP64 one (default: the
+    same)."""
+    kernel64 = kernel if kernel64 is None else kernel64
+    kw64 = kw if kw64 is None else kw64
     import ctypes as C
     import torch
     from sbb._lib import lib
@@ -412,7 +417,7 @@ def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local):
     rp = torch.from_numpy(A.rowptr32()).to(dev)
     col = torch.from_numpy(A.col).to(dev)
     y0 = torch.from_numpy(y_h).to(dev)
-    P64 = Plan(rp, col, torch.from_numpy(A.val).to(dev), n, kernel=kernel, **kw)
+    P64 = Plan(rp, col, torch.from_numpy(A.val).to(dev), n, kernel=kernel64, **kw64)
     P32 = Plan(rp, col, torch.from_numpy(A.val.astype(np.float32)).to(dev), n, kernel=kernel,
                f32=True, **kw)
     x64 = torch.from_numpy(x_h).to(dev)
@@ -449,13 +454,14 @@ def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local):
     ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x_h, alpha, beta, y_h)
     err = np.abs(got - ref) / np.where(sc > 0, sc, 1.0)
     info = P32.info()
+    info64 = P64.info()
     launches = lib().sbb_plan_launches(P32.h)
     P64.close()
     P32.close()
     return dict(step64=step64, kern64=kern64, step32=step32, kern32=kern32,
                 err_max=float(err.max()), err_median=float(np.median(err)), info=info,
-                launches=launches,
-                tag=KERNEL_TAGS[info["kernel"]])
+                info64=info64, launches=launches,
+                tag=KERNEL_TAGS[info["kernel"]], tag64=KERNEL_TAGS[info64["kernel"]])
 
 
 def run_f32(args, ws, rank, local):
@@ -464,9 +470,14 @@ def run_f32(args, ws, rank, local):
     m, n, nnz = A.m, A.n, A.nnz
     bytes64 = algo_bytes(m, n, nnz)
     bytes32 = 8 * nnz + 4 * (m + 1) + 4 * n + 16 * m
-    kw = dict(tile_sigma=args.sigma) if args.kernel == "tiled" else {}
+    # The FP64 side is the plain path as the default line runs it (the tiled
+    # kernel, sigma 4); the FP32 side uses its own automatic choice (32 x 8
+    # tiles) unless --kernel / --sigma say otherwise.
+    kw = dict(tile_sigma=args.sigma) if args.kernel == "tiled" and args.sigma_given else {}
+    kernel32 = args.kernel if args.sigma_given or args.kernel != "tiled" else "auto"
     with ClockSampler(local) as clk:
-        r = f32_measure(A, x_h, y_h, alpha, beta, args.kernel, kw, args.warmup, args.steps, local)
+        r = f32_measure(A, x_h, y_h, alpha, beta, kernel32, kw, args.warmup, args.steps, local,
+                        kernel64="tiled", kw64=dict(tile_sigma=4))
     ms32 = max_over_ranks(r["step32"], ws)
     peak, peak_kind = peaks()
     if rank == 0:
@@ -482,6 +493,7 @@ def run_f32(args, ws, rank, local):
                        "nnz": nnz, "kernel": r["tag"], "plan": {k: r["info"][k] for k in
                                                                 ("tile_sigma", "vector_width",
                                                                  "items_per_thread")},
+                       "fp64_kernel": r["tag64"], "fp64_tile_sigma": r["info64"]["tile_sigma"],
                        "fp64_plan_ms_per_step": round(r["step64"], 5),
                        "fp64_kernel_ms": round(r["kern64"], 5),
                        "f32_kernel_ms": round(r["kern32"], 5),
@@ -616,10 +628,14 @@ def extra_configs(A2, x2, y2, local, cpu_budget):
     f = {}
     for name, (A, x_h, y_h, alpha, beta) in (("c1_matrix", make_workload("c1")[:5]),
                                              ("c2_matrix", (A2, x2, y2, 1.0, 0.5))):
-        r = f32_measure(A, x_h, y_h, alpha, beta, "auto", {}, 10, 100, local)
+        r = f32_measure(A, x_h, y_h, alpha, beta, "auto", {}, 10, 100, local,
+                        kernel64="tiled" if name == "c2_matrix" else "auto",
+                        kw64=dict(tile_sigma=4) if name == "c2_matrix" else {})
         b64 = algo_bytes(A.m, A.n, A.nnz)
         b32 = 8 * A.nnz + 4 * (A.m + 1) + 4 * A.n + 16 * A.m
-        f[name] = {"kernel": r["tag"], "fp64_kernel_ms": round(r["kern64"], 5),
+        f[name] = {"kernel": r["tag"], "tile_sigma": r["info"]["tile_sigma"],
+                   "fp64_kernel": r["tag64"], "fp64_tile_sigma": r["info64"]["tile_sigma"],
+                   "fp64_kernel_ms": round(r["kern64"], 5),
                    "f32_kernel_ms": round(r["kern32"], 5),
                    "fp64_step_ms": round(r["step64"], 5), "f32_step_ms": round(r["step32"], 5),
                    "speedup_kernel_vs_fp64": round(r["kern64"] / r["kern32"], 3),
@@ -843,7 +859,8 @@ def main():
                     choices=["merge", "vector", "tiled", "rows", "auto"])
     ap.add_argument("--ipt", type=int, default=6)
     ap.add_argument("--persistent", type=int, default=0)
-    ap.add_argument("--sigma", type=int, default=4, help="tiled kernel: nnz per lane (0 = CSR5 rule)")
+    ap.add_argument("--sigma", type=int, default=None,
+                    help="tiled kernel: nnz per lane (0 = CSR5 rule; default 4)")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -854,6 +871,9 @@ def main():
     ap.add_argument("--f32", action="store_true",
                     help="time the FP32-storage compensated form against the FP64 plan")
     args = ap.parse_args()
+    args.sigma_given = args.sigma is not None
+    if args.sigma is None:
+        args.sigma = 4
     if args.warmup < 3:
         args.warmup = 3
     if args.mtx:

@@ -289,17 +289,17 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
         return ok;
     };
     int b = 0;
-    // Tiles of sigma >= 8 load y of the segments they can write before the
+    // Tiles of sigma >= 16 load y of the segments they can write before the
     // tile arrives, from the segment ranks of this tile and the next one.
     int tseg = 0, tseg1 = 0;
-    if (SIGMA >= 8 && t < tiles) {
+    if (SIGMA >= kTileStagedSigma && t < tiles) {
         tseg = __ldg(tile_seg + t);
         tseg1 = __ldg(tile_seg + t + 1);
     }
     for (; t < tiles; t += W) {
         double ya = 0.0, yb = 0.0;
         int tseg_n = 0, tseg1_n = 0;
-        if (SIGMA >= 8) {
+        if (SIGMA >= kTileStagedSigma) {
             if (beta != 0.0) {
                 const int lim = tseg1 + (t + 1 < tiles ? 1 : 0);
                 if (tseg + lane < lim)

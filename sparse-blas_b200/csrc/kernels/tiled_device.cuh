@@ -33,11 +33,14 @@ __host__ __device__ constexpr size_t tile_bytes_of(int sigma, int vbytes)
     return tile_hdr_offset(sigma, vbytes) + tile_hdr_bytes(sigma);
 }
 constexpr unsigned kTileCloses = 1u, kTileStartsRow = 2u;
-// Per-warp staging of a tile's row sums: up to 32*sigma + 1 segments (only
-// tiles of sigma >= 8 stage them).
+// Tiles of at least this sigma stage their row sums in shared memory and
+// write them in one coalesced pass; smaller tiles write each row as it
+// completes.
+constexpr int kTileStagedSigma = 16;
+// Per-warp staging of a tile's row sums: up to 32*sigma + 1 segments.
 __host__ __device__ constexpr size_t sum_bytes_of(int sigma)
 {
-    return sigma < 8 ? 0 : ((size_t)(32 * sigma + 1) * 8 + 127) / 128 * 128;
+    return sigma < kTileStagedSigma ? 0 : ((size_t)(32 * sigma + 1) * 8 + 127) / 128 * 128;
 }
 
 // ---- TMA (1-D bulk async copy) helpers ------------------------------------
@@ -133,11 +136,11 @@ __device__ __forceinline__ void tile_gather(int t, int tiles, long long nnz, con
 
 // Reduces one tile whose x values are already gathered (xv).  The tile's
 // segment rank, closing flag and each lane's count of earlier row starts come
-// from its header.  Tiles of sigma >= 8 stage row sums in the warp's s_sum
+// from its header.  Tiles of sigma >= 16 stage row sums in the warp's s_sum
 // (index = segment - tseg) and write them to y in one coalesced pass at the
 // end, so the divergent per-nnz loop touches no global memory; ya/yb hold y
 // of segments tseg+lane and tseg+32+lane, loaded when the tile started.
-// Tiles of sigma < 8 write each row as it completes.
+// Tiles of sigma 4 and 8 write each row as it completes.
 template <typename PT, typename ACC, int SIGMA>
 __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
                                             const int *__restrict__ ne,
@@ -170,10 +173,12 @@ __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
     else
         excl = reinterpret_cast<const unsigned short *>(tb + HDR + 16)[lane];
 
-    // 2. segment rows of this lane.  Tiles of sigma >= 8 stage row sums and
-    // write them in one coalesced pass; sigma = 4 tiles (few rows per lane,
-    // tightest register budget) write each row as it completes.
-    constexpr bool kStaged = SIGMA >= 8;
+    // 2. segment rows of this lane.  Tiles of sigma >= 16 stage row sums and
+    // write them in one coalesced pass; sigma 4 and 8 tiles (few rows per
+    // lane, tight register budgets) write each row as it completes, which
+    // measured faster for them (sigma 8: 0.130 vs 0.196 ms, FP32 storage, on
+    // the 5.5M-row matrix).
+    constexpr bool kStaged = SIGMA >= kTileStagedSigma;
     auto put = [&](int sg, double sum) {
         if (kStaged) {
             s_sum[sg - tseg] = sum;
