@@ -583,11 +583,40 @@ def plain_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, reps, local):
     P.check()
     kern = statistics.median(ev[2 + 2 * i].elapsed_time(ev[3 + 2 * i]) for i in range(reps))
     step = ev[0].elapsed_time(ev[1]) / reps
+    graph = graph_step_ms(P, x, y, alpha, beta, min(reps, 100))
     info = P.info()
     launches = lib().sbb_plan_launches(P.h)
     P.close()
-    return dict(kernel_ms=kern, step_ms=step, plan_build_ms=build_ms, info=info,
-                launches=launches)
+    return dict(kernel_ms=kern, step_ms=step, graph_step_ms=graph, plan_build_ms=build_ms,
+                info=info, launches=launches)
+
+
+def graph_step_ms(P, x, y, alpha, beta, steps):
+    """ms per SpMV with `steps` SpMVs of the plan captured in one CUDA graph
+    and replayed: the device time of a step without the host's launch work
+    between steps (which dominates the host-launched step time of small
+    matrices)."""
+    import torch
+    try:
+        g = torch.cuda.CUDAGraph()
+        cs = torch.cuda.Stream()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=cs):
+            for _ in range(steps):
+                P.spmv(x, y, alpha, beta)
+        g.replay()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        del g
+        return ms
+    except Exception:  # a measurement aid only
+        return None
 
 
 def config_line(name, kernel, kw, local, cpu_budget, reps=200):
@@ -606,6 +635,9 @@ def config_line(name, kernel, kw, local, cpu_budget, reps=200):
             "plan": {k: r["info"][k] for k in ("vector_width", "items_per_thread",
                                                "tile_sigma", "tiles")},
             "step_ms": round(r["step_ms"], 5), "kernel_ms": round(r["kernel_ms"], 5),
+            "graph_step_ms": (round(r["graph_step_ms"], 5) if r["graph_step_ms"] else None),
+            "graph_GB/s": (round(b / (r["graph_step_ms"] * 1e-3) / 1e9, 2)
+                           if r["graph_step_ms"] else None),
             "GB/s": round(b / (r["step_ms"] * 1e-3) / 1e9, 2),
             "GFLOP/s": round(fl / (r["step_ms"] * 1e-3) / 1e9, 2),
             "kernel_GB/s": round(b / (r["kernel_ms"] * 1e-3) / 1e9, 2),

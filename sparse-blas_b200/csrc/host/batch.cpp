@@ -271,6 +271,24 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
     };
     cudaError_t e;
     const int nfix = (int)fix_mat.size(), nruns = (int)run_mat.size();
+    // long runs first: the fix-up gives them whole blocks, short runs a warp
+    int n_long_runs = 0;
+    {
+        std::vector<int> order(nruns);
+        for (int i = 0; i < nruns; ++i) order[i] = i;
+        std::stable_partition(order.begin(), order.end(),
+                              [&](int i) { return run_len[i] > kWarpRunMax; });
+        std::vector<int> rm(nruns), rf(nruns), rl(nruns);
+        for (int i = 0; i < nruns; ++i) {
+            rm[i] = run_mat[order[i]];
+            rf[i] = run_first[order[i]];
+            rl[i] = run_len[order[i]];
+            n_long_runs += rl[i] > kWarpRunMax;
+        }
+        run_mat.swap(rm);
+        run_first.swap(rf);
+        run_len.swap(rl);
+    }
     const int nempty = (int)empty_row.size();
     for (int f = 0; f < kBatchFamilies; f++) {
         const size_t nf = fmats[f].size();
@@ -312,8 +330,9 @@ int sbb_batch_create(sbb_batch_t *out, const sbb_batch_item *items, int count, v
         (e = cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s)) ||
         (e = cudaStreamSynchronize(s)))
         return fail(e);
-    b->fix = BatchFix{b->d_tile0,   b->d_fix_mat, nfix,           b->d_run_mat,   b->d_run_first,
-                      b->d_run_len, nruns,        b->d_empty_row, b->d_empty_mat, nempty};
+    b->fix = BatchFix{b->d_tile0,   b->d_fix_mat, nfix,        b->d_run_mat,   b->d_run_first,
+                      b->d_run_len, nruns,        n_long_runs, b->d_empty_row, b->d_empty_mat,
+                      nempty};
     b->fix_slots = tile0.back();
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);

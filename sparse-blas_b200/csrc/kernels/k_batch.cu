@@ -226,11 +226,12 @@ batch_kernel(const BatchMat *__restrict__ mats, int nmat, const long long *__res
 // The standalone fix-up (k_fixup.cu) and empty-row pass (k_tiled.cu) over
 // every merge/tiled matrix of the batch at once, with the same arithmetic:
 // blocks [0, short_blocks) take one global carry slot per thread (single
-// carries), the next n_runs blocks one multi-slot run each, the rest the empty
-// rows of tiled matrices.
+// carries), the next n_long_runs blocks one long run each (more than
+// kWarpRunMax slots), the next warp_blocks eight short runs each (a warp a
+// run), the rest the empty rows of tiled matrices.
 __global__ void __launch_bounds__(kFixupThreads)
 batch_fixup_kernel(const BatchMat *__restrict__ mats, BatchFix F, long long total_slots,
-                   int short_blocks)
+                   int short_blocks, int warp_blocks)
 {
     if (blockIdx.x < short_blocks) {
         const long long g = (long long)blockIdx.x * kFixupThreads + threadIdx.x;
@@ -246,7 +247,16 @@ batch_fixup_kernel(const BatchMat *__restrict__ mats, BatchFix F, long long tota
         return;
     }
     const int j = blockIdx.x - short_blocks;
-    if (j < F.n_runs) {
+    if (j >= F.n_long_runs && j < F.n_long_runs + warp_blocks) {
+        const int q = F.n_long_runs + (j - F.n_long_runs) * (kFixupThreads / 32) + (threadIdx.x >> 5);
+        if (q >= F.n_runs) return;
+        const BatchMat &M = mats[__ldg(F.run_mat + q)];
+        const int first = __ldg(F.run_first + q), len = __ldg(F.run_len + q);
+        const double sum = fixup_run_warp(M.carry_val, first, len);
+        if ((threadIdx.x & 31) == 0) fixup_single(M.y, M.crow[first], M.alpha, sum);
+        return;
+    }
+    if (j < F.n_long_runs) {
         __shared__ double s[kFixupThreads];
         const BatchMat &M = mats[__ldg(F.run_mat + j)];
         const int first = __ldg(F.run_first + j), len = __ldg(F.run_len + j);
@@ -259,7 +269,7 @@ batch_fixup_kernel(const BatchMat *__restrict__ mats, BatchFix F, long long tota
         if (threadIdx.x == 0) fixup_single(M.y, M.crow[first], M.alpha, s[0]);
         return;
     }
-    const long long e = (long long)(j - F.n_runs) * kFixupThreads + threadIdx.x;
+    const long long e = (long long)(j - F.n_long_runs - warp_blocks) * kFixupThreads + threadIdx.x;
     if (e >= F.n_empty) return;
     const BatchMat &M = mats[__ldg(F.empty_mat + e)];
     double *yp = M.y + __ldg(F.empty_row + e);
@@ -313,8 +323,9 @@ void launch_batch_fixup(const BatchMat *mats, const BatchFix &F, long long total
     if (total_slots <= 0 && F.n_empty <= 0) return;
     const int short_blocks = (int)((total_slots + kFixupThreads - 1) / kFixupThreads);
     const int empty_blocks = (F.n_empty + kFixupThreads - 1) / kFixupThreads;
-    batch_fixup_kernel<<<short_blocks + F.n_runs + empty_blocks, kFixupThreads, 0, s>>>(
-        mats, F, total_slots, short_blocks);
+    const int warp_blocks = (F.n_runs - F.n_long_runs + kFixupThreads / 32 - 1) / (kFixupThreads / 32);
+    batch_fixup_kernel<<<short_blocks + F.n_long_runs + warp_blocks + empty_blocks, kFixupThreads, 0, s>>>(
+        mats, F, total_slots, short_blocks, warp_blocks);
 }
 
 }  // namespace sbb

@@ -7,11 +7,15 @@
 // tiling, so it is fixed when the plan is built; so are the runs of
 // consecutive tiles carrying the same row (a long row spans many tiles).
 //
-// Run time: one launch.  The first blocks take one multi-tile run each and
-// add its carries summed in a fixed order (per-thread strided sums, then a
-// shared-memory tree); the other blocks stride over the tiles and add
-// single-tile carries.  Each row is updated by one thread, so results are
+// Run time: one launch.  The first blocks take one long run each (more than
+// kWarpRunMax carries: per-thread strided sums, then a shared-memory tree),
+// the next take eight short runs each (one warp a run: lane-strided sums,
+// then a butterfly), the others stride over the tiles and add single-tile
+// carries.  Each row is updated by one thread, so results are
 // bit-reproducible.
+#include <algorithm>
+#include <vector>
+
 #include "../sbb_internal.h"
 #include "spmv_device.cuh"
 
@@ -58,15 +62,27 @@ __global__ void runs_mark_kernel(const int *__restrict__ crow, int T, int m,
     run_len[j] = lo - t + 1;
 }
 
-// Blocks [0, long_blocks) take the multi-tile runs (launched first: they
-// are the longest); the rest stride over the tiles for single carries.
+// Blocks [0, long_blocks) take the long runs (launched first: they are the
+// longest), the next warp_blocks the short runs, eight per block; the rest
+// stride over the tiles for single carries.  With a device-side run count
+// (dev_count), the long_blocks stride over every run.
 __global__ void __launch_bounds__(FT)
 fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cval, int T,
              const int *__restrict__ run_first, const int *__restrict__ run_len, int long_blocks,
-             double alpha, double *__restrict__ y, unsigned *queue, const int *dev_count)
+             int n_long, int n_runs_host, int warp_blocks, double alpha, double *__restrict__ y,
+             unsigned *queue, const int *dev_count)
 {
+    if (blockIdx.x >= long_blocks && blockIdx.x < long_blocks + warp_blocks) {
+        const int j = n_long + (blockIdx.x - long_blocks) * (FT / 32) + (threadIdx.x >> 5);
+        if (j >= n_runs_host) return;
+        const int first = run_first[j], len = run_len[j];
+        const double sum = fixup_run_warp(cval, first, len);
+        if ((threadIdx.x & 31) == 0) fixup_single(y, crow[first], alpha, sum);
+        return;
+    }
     if (blockIdx.x >= long_blocks) {
-        const int sb = blockIdx.x - long_blocks, nsb = gridDim.x - long_blocks;
+        const int sb = blockIdx.x - long_blocks - warp_blocks,
+                  nsb = gridDim.x - long_blocks - warp_blocks;
         if (sb == 0 && threadIdx.x == 0 && queue != nullptr) queue[0] = 0u;  // rearm a work queue
         for (int t = sb * FT + threadIdx.x; t < T; t += nsb * FT) {
             const int r = crow[t];
@@ -78,7 +94,7 @@ fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cva
     }
     __shared__ double s[FT];
     // with a device-side count, a fixed set of blocks strides over the runs
-    const int n_runs = dev_count ? *dev_count : long_blocks;
+    const int n_runs = dev_count ? *dev_count : n_long;
     for (int j = blockIdx.x; j < n_runs; j += long_blocks) {
         const int first = run_first[j], len = run_len[j];
         s[threadIdx.x] = fixup_partial(cval, first, len, threadIdx.x);
@@ -115,6 +131,26 @@ int carry_runs_build(const int *crow, int T, int m, CarryRuns *R, cudaStream_t s
     SBB_CUDA(cudaStreamSynchronize(s));
     SBB_CUDA(cudaFreeAsync(count, s));
     R->n_runs = h;
+    R->n_long = 0;
+    if (h > 0) {  // long runs first (the fix-up gives them whole blocks)
+        std::vector<int> f(h), l(h);
+        SBB_CUDA(cudaMemcpyAsync(f.data(), R->run_first, sizeof(int) * h, cudaMemcpyDeviceToHost, s));
+        SBB_CUDA(cudaMemcpyAsync(l.data(), R->run_len, sizeof(int) * h, cudaMemcpyDeviceToHost, s));
+        SBB_CUDA(cudaStreamSynchronize(s));
+        std::vector<int> order(h);
+        for (int i = 0; i < h; ++i) order[i] = i;
+        std::stable_partition(order.begin(), order.end(),
+                              [&](int i) { return l[i] > kWarpRunMax; });
+        std::vector<int> f2(h), l2(h);
+        for (int i = 0; i < h; ++i) {
+            f2[i] = f[order[i]];
+            l2[i] = l[order[i]];
+            R->n_long += l2[i] > kWarpRunMax;
+        }
+        SBB_CUDA(cudaMemcpyAsync(R->run_first, f2.data(), sizeof(int) * h, cudaMemcpyHostToDevice, s));
+        SBB_CUDA(cudaMemcpyAsync(R->run_len, l2.data(), sizeof(int) * h, cudaMemcpyHostToDevice, s));
+        SBB_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    }
     return SBB_OK;
 }
 
@@ -129,6 +165,7 @@ void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async)
         }
     R->run_first = R->run_len = nullptr;
     R->n_runs = 0;
+    R->n_long = 0;
 }
 
 void launch_runs_mark(const int *crow, int T, int m, int *run_first, int *run_len,
@@ -145,10 +182,11 @@ void launch_fixup(int m, const int *crow, const double *cval, int T, const Carry
     // single carries: one wave of blocks at most, each thread striding over tiles
     int short_blocks = (T + FT - 1) / FT;
     if (short_blocks > 148 * 8) short_blocks = 148 * 8;
-    const int long_blocks = dev_count ? 148 : R.n_runs;
-    fixup_kernel<<<short_blocks + long_blocks, FT, 0, s>>>(m, crow, cval, T, R.run_first,
-                                                           R.run_len, long_blocks, alpha, y,
-                                                           queue, dev_count);
+    const int long_blocks = dev_count ? 148 : R.n_long;
+    const int warp_blocks = dev_count ? 0 : (R.n_runs - R.n_long + FT / 32 - 1) / (FT / 32);
+    fixup_kernel<<<short_blocks + long_blocks + warp_blocks, FT, 0, s>>>(
+        m, crow, cval, T, R.run_first, R.run_len, long_blocks, R.n_long, R.n_runs, warp_blocks,
+        alpha, y, queue, dev_count);
 }
 
 }  // namespace sbb

@@ -423,13 +423,9 @@ void launch_rows_n(const RowsPlan &R, const Plan *p, double alpha, const typenam
     using V = typename PT::V;
     auto kern = rows_kernel<PT, NMAX, MINB>;
     constexpr size_t smem = (size_t)RW * kNbuf * RowsSlot<V, NMAX>::BYTES;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 148, occ = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, RW * 32, smem);
+    const LaunchShape ls = cached_launch_shape(kern, RW * 32, smem);
     const long long want = (R.nblk + RW - 1) / RW;
-    const long long cap = (long long)sms * (occ > 0 ? occ : 1);
+    const long long cap = (long long)ls.sms * ls.occ;
     const int grid = (int)(want < cap ? want : cap);
     hook_start(s);
     kern<<<grid, RW * 32, smem, s>>>(R.nblk, R.desc, p->rowptr, p->col,

@@ -354,11 +354,14 @@ struct TiledTuning {
 };
 static TiledTuning tiled_tuning()
 {
-    TiledTuning t{2, 1};
-    if (const char *e = getenv("SBB_TILED_STAGES")) t.stages = atoi(e);
-    if (const char *e = getenv("SBB_TILED_EVICT_FIRST")) t.evict_first = atoi(e);
-    if (t.stages < 2 || t.stages > 4) t.stages = 2;
-    return t;
+    static const TiledTuning tuning = [] {  // read once per process
+        TiledTuning t{2, 1};
+        if (const char *e = getenv("SBB_TILED_STAGES")) t.stages = atoi(e);
+        if (const char *e = getenv("SBB_TILED_EVICT_FIRST")) t.evict_first = atoi(e);
+        if (t.stages < 2 || t.stages > 4) t.stages = 2;
+        return t;
+    }();
+    return tuning;
 }
 
 template <typename PT, typename ACC, int SIGMA, int NBUF>
@@ -369,13 +372,9 @@ void launch_tiled_n(const TiledPlan &T, int m, int n, long long nnz, double alph
     auto kern = tiled_kernel<PT, ACC, SIGMA, NBUF>;
     constexpr size_t smem =
         (size_t)TW * (NBUF * tile_bytes_of(SIGMA, sizeof(typename PT::V)) + sum_bytes_of(SIGMA));
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 148, occ = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TW * 32, smem);
+    const LaunchShape ls = cached_launch_shape(kern, TW * 32, smem);
     long long want = (T.tiles + TW - 1) / TW;
-    long long cap = (long long)sms * (occ > 0 ? occ : 1);
+    long long cap = (long long)ls.sms * ls.occ;
     int grid = (int)(want < cap ? want : cap);
     hook_start(s);
     kern<<<grid, TW * 32, smem, s>>>(m, n, nnz, T.tiles, T.blob, T.tile_seg, T.ne, x, y, alpha,

@@ -100,8 +100,11 @@ __device__ __forceinline__ void vector_chunk(int r0, int m, int n, const int *__
 
 // Carry fix-up arithmetic shared by the standalone fix-up (k_fixup.cu) and
 // the batch fix-up (k_batch.cu): a single carry is added as fma(alpha, c, y[r]); a
-// run of carries is summed by kFixupThreads threads (thread i: slots i,
-// i + kFixupThreads, ... in order) and then by a shared-memory tree.
+// run of at most kWarpRunMax carries is summed by one warp (lane i: slots i,
+// i + 32, ... in order, then an xor butterfly); a longer run by kFixupThreads
+// threads (thread i: slots i, i + kFixupThreads, ... in order) and then a
+// shared-memory tree.  Which of the two a run gets depends only on its
+// length, so both fix-ups sum every run in the same order.
 constexpr int kFixupThreads = 256;
 __device__ __forceinline__ void fixup_single(double *y, int r, double alpha, double c)
 {
@@ -119,6 +122,15 @@ __device__ __forceinline__ double warp_sum(double v)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// Sum of a run of at most kWarpRunMax carries by the calling warp (every lane
+// gets it).
+__device__ __forceinline__ double fixup_run_warp(const double *cval, int first, int len)
+{
+    double acc = 0.0;
+    for (int i = threadIdx.x & 31; i < len; i += 32) acc += cval[first + i];
+    return warp_sum(acc);
 }
 
 // Sum of the products s_p[lo..hi) by the whole warp (fixed order: lane-strided

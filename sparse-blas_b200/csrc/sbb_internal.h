@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 #include "sbb_spmv.h"
@@ -49,6 +50,37 @@ enum : unsigned {
     ST_TIMEOUT = 1u << 4,      // a bounded wait on a copy gave up
 };
 
+// Resident CTAs per SM and SM count for a persistent kernel with the given
+// block size and dynamic shared memory, on the current device.  The occupancy
+// query runs once per device and kernel and later launches read the cache
+// (the host work per launch otherwise shows up as idle GPU time between
+// short SpMVs); the shared-memory attribute, which a new context would not
+// have, is set on every launch that needs more than the default 48 KB.
+struct LaunchShape {
+    int sms, occ;
+};
+template <typename K>
+LaunchShape cached_launch_shape(K kern, int threads, size_t smem)
+{
+    static std::atomic<long long> cache[64];  // sms << 32 | occ, 0 = not yet known
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    long long v = cache[dev].load(std::memory_order_acquire);
+    if (v == 0) {  // racing first calls compute the same value
+        int sms = 148, occ = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+        if (sms < 1) sms = 1;
+        if (occ < 1) occ = 1;
+        v = ((long long)sms << 32) | occ;
+        cache[dev].store(v, std::memory_order_release);
+    }
+    return LaunchShape{(int)(v >> 32), (int)(v & 0xffffffff)};
+}
+
 // ---- kernel launchers (defined in the .cu files) ---------------------------
 constexpr int kMergeThreads = 256;
 // Tile plans take at most this many rows: row counts and segment ranks plus
@@ -79,9 +111,13 @@ void launch_vector_f32(const CsrView &A, int V, double alpha, const float *x,
 // Per-tile carries: carry_row[t] (static per plan; m = nothing carried) and
 // carry_val[t] (written by the tiled kernel).  Runs of >= 2 tiles carrying
 // the same row are listed once at plan time.
+// Runs of at most this many carries are summed by one warp, longer ones by a
+// block (spmv_device.cuh: fixup_run_warp, fixup_partial).
+constexpr int kWarpRunMax = 1024;
 struct CarryRuns {
     int *run_first = nullptr, *run_len = nullptr;
     int n_runs = 0;
+    int n_long = 0;   // runs longer than kWarpRunMax, listed first
     size_t bytes = 0;
 };
 int carry_runs_build(const int *carry_row, int T, int m, CarryRuns *R, cudaStream_t s);
@@ -151,8 +187,9 @@ struct BatchFix {
     const long long *tile0;          // nfix+1: first global carry slot of each matrix with slots
     const int *mat;                  // nfix: batch index of each such matrix
     int nfix;
-    const int *run_mat, *run_first, *run_len;  // multi-slot runs (all matrices)
-    int n_runs;
+    const int *run_mat, *run_first, *run_len;  // multi-slot runs (all matrices),
+    int n_runs;                                // those longer than kWarpRunMax first
+    int n_long_runs;
     const int *empty_row, *empty_mat;          // empty rows of tiled matrices: y = beta*y
     int n_empty;
 };

@@ -459,3 +459,33 @@ def test_unaligned_views(cuda, f32):
                 P.close()
                 tol = 1e-12 if not f32 else 1e-12
                 assert max_scaled_err(yy.cpu().numpy(), y_ref, sc) <= tol, (kernel, off_i, off_v)
+
+
+@pytest.mark.parametrize("cfg", [dict(kernel="tiled", tile_sigma=4), dict(kernel="tiled", tile_sigma=16),
+                                 dict(kernel="merge", items_per_thread=8), dict(kernel="rows"),
+                                 dict(kernel="vector", vector_width=8)])
+def test_plan_spmv_captured_in_cuda_graph(cuda, cfg):
+    """A plan's SpMVs captured in a CUDA graph and replayed give the same bits
+    as the same calls launched directly (after one direct call on the device,
+    which sets the launch configuration up)."""
+    import torch
+    from sbb.device import Plan
+    rp, col, val, x, y = MATS["long_rows"]()
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    P = Plan(drp, dcol, dval, len(x), **cfg)
+    y_direct = dy.clone()
+    for _ in range(3):
+        P.spmv(dx, y_direct, 1.1, 0.7)
+    torch.cuda.synchronize()
+    y_graph = dy.clone()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=torch.cuda.Stream()):
+        for _ in range(3):
+            P.spmv(dx, y_graph, 1.1, 0.7)
+    y_graph.copy_(dy)
+    g.replay()
+    torch.cuda.synchronize()
+    P.check()
+    assert torch.equal(y_graph, y_direct)
+    del g
+    P.close()
