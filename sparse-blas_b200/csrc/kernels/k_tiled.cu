@@ -237,7 +237,7 @@ template <int SIGMA> struct TiledShape {
 // warps), fixed per launch shape, so results do not depend on timing.  Each
 // warp keeps a ring of NBUF tile blobs in shared memory: lane 0 issues the
 // bulk copy of tile i+NBUF as soon as tile i is reduced.
-template <typename PT, typename ACC, int SIGMA, int NBUF>
+template <typename PT, typename ACC, int SIGMA, int NBUF, bool NE>
 __global__ void __launch_bounds__(TW * 32, TiledShape<SIGMA>::MINB)
 tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__restrict__ blob,
              const int *__restrict__ tile_seg, const int *__restrict__ ne,
@@ -303,9 +303,10 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
             if (beta != 0.0) {
                 const int lim = tseg1 + (t + 1 < tiles ? 1 : 0);
                 if (tseg + lane < lim)
-                    ya = ld_y(y + (ne ? __ldg(ne + tseg + lane) : tseg + lane), streaming);
+                    ya = ld_y(y + (NE && ne ? __ldg(ne + tseg + lane) : tseg + lane), streaming);
                 if (tseg + 32 + lane < lim)
-                    yb = ld_y(y + (ne ? __ldg(ne + tseg + 32 + lane) : tseg + 32 + lane), streaming);
+                    yb = ld_y(y + (NE && ne ? __ldg(ne + tseg + 32 + lane) : tseg + 32 + lane),
+                              streaming);
             }
             const int tn = t + W;  // segment ranks of the next tile, in flight meanwhile
             if (tn < tiles) {
@@ -319,7 +320,7 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
         }
         V xv[SIGMA];
         tile_gather<PT, SIGMA>(t, tiles, nnz, wbuf + b * TB, x, keep, xv);
-        tile_reduce<PT, ACC, SIGMA>(t, wbuf + b * TB, ne, xv, y, alpha, beta, carry_val, streaming,
+        tile_reduce<PT, ACC, SIGMA, NE>(t, wbuf + b * TB, ne, xv, y, alpha, beta, carry_val, streaming,
                                     ya, yb, s_sum);
         __syncwarp();  // every lane is done with buffer b before it is refilled
         if (lane == 0 && t + NBUF * W < tiles) issue(t + NBUF * W, b);
@@ -347,38 +348,33 @@ int grid_for(long long work, int tpb)
     return (int)g;
 }
 
-// Pipeline depth (tile blobs in flight per warp) and the L2 policy of the
-// bulk copies; SBB_TILED_STAGES / SBB_TILED_EVICT_FIRST override the defaults.
-struct TiledTuning {
-    int stages, evict_first;
-};
-static TiledTuning tiled_tuning()
+// L2 policy of the bulk copies (SBB_TILED_EVICT_FIRST=0 turns the
+// evict-first hint off), read once per process.  Deeper copy rings (3-4
+// tiles per warp) measured slower and are not built.
+static int tiled_evict_first()
 {
-    static const TiledTuning tuning = [] {  // read once per process
-        TiledTuning t{2, 1};
-        if (const char *e = getenv("SBB_TILED_STAGES")) t.stages = atoi(e);
-        if (const char *e = getenv("SBB_TILED_EVICT_FIRST")) t.evict_first = atoi(e);
-        if (t.stages < 2 || t.stages > 4) t.stages = 2;
-        return t;
+    static const int v = [] {
+        const char *e = getenv("SBB_TILED_EVICT_FIRST");
+        return e ? atoi(e) : 1;
     }();
-    return tuning;
+    return v;
 }
 
-template <typename PT, typename ACC, int SIGMA, int NBUF>
+template <typename PT, typename ACC, int SIGMA, bool NE>
 void launch_tiled_n(const TiledPlan &T, int m, int n, long long nnz, double alpha,
                     const typename PT::V *x, double beta, double *y, unsigned *status,
-                    int evict_first, cudaStream_t s)
+                    cudaStream_t s)
 {
-    auto kern = tiled_kernel<PT, ACC, SIGMA, NBUF>;
+    auto kern = tiled_kernel<PT, ACC, SIGMA, 2, NE>;
     constexpr size_t smem =
-        (size_t)TW * (NBUF * tile_bytes_of(SIGMA, sizeof(typename PT::V)) + sum_bytes_of(SIGMA));
+        (size_t)TW * (2 * tile_bytes_of(SIGMA, sizeof(typename PT::V)) + sum_bytes_of(SIGMA));
     const LaunchShape ls = cached_launch_shape(kern, TW * 32, smem);
     long long want = (T.tiles + TW - 1) / TW;
     long long cap = (long long)ls.sms * ls.occ;
     int grid = (int)(want < cap ? want : cap);
     hook_start(s);
     kern<<<grid, TW * 32, smem, s>>>(m, n, nnz, T.tiles, T.blob, T.tile_seg, T.ne, x, y, alpha,
-                                     beta, T.carry_val, status, evict_first,
+                                     beta, T.carry_val, status, tiled_evict_first(),
                                      first_wait_budget());
     hook_stop(s);
 }
@@ -388,13 +384,10 @@ void launch_tiled_s(const TiledPlan &T, int m, int n, long long nnz, double alph
                     const typename PT::V *x, double beta, double *y, unsigned *status,
                     cudaStream_t s)
 {
-    const TiledTuning tu = tiled_tuning();
-    if (SIGMA <= 8 && tu.stages == 3)
-        launch_tiled_n<PT, ACC, SIGMA, 3>(T, m, n, nnz, alpha, x, beta, y, status, tu.evict_first, s);
-    else if (SIGMA <= 8 && tu.stages == 4)
-        launch_tiled_n<PT, ACC, SIGMA, 4>(T, m, n, nnz, alpha, x, beta, y, status, tu.evict_first, s);
+    if (T.ne)
+        launch_tiled_n<PT, ACC, SIGMA, true>(T, m, n, nnz, alpha, x, beta, y, status, s);
     else
-        launch_tiled_n<PT, ACC, SIGMA, 2>(T, m, n, nnz, alpha, x, beta, y, status, tu.evict_first, s);
+        launch_tiled_n<PT, ACC, SIGMA, false>(T, m, n, nnz, alpha, x, beta, y, status, s);
 }
 
 template <typename PT, typename ACC>

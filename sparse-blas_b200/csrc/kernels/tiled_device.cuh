@@ -141,7 +141,8 @@ __device__ __forceinline__ void tile_gather(int t, int tiles, long long nnz, con
 // end, so the divergent per-nnz loop touches no global memory; ya/yb hold y
 // of segments tseg+lane and tseg+32+lane, loaded when the tile started.
 // Tiles of sigma 4 and 8 write each row as it completes.
-template <typename PT, typename ACC, int SIGMA>
+// NE = false: the matrix has no empty rows (ne is null), segment = row.
+template <typename PT, typename ACC, int SIGMA, bool NE = true>
 __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
                                             const int *__restrict__ ne,
                                             const typename PT::V (&xv)[SIGMA],
@@ -183,7 +184,7 @@ __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
         if (kStaged) {
             s_sum[sg - tseg] = sum;
         } else {
-            write_y(y + (ne ? __ldg(ne + sg) : sg), alpha, sum, beta, stream);
+            write_y(y + (NE && ne ? __ldg(ne + sg) : sg), alpha, sum, beta, stream);
         }
     };
     const int head_seg = tseg - (int)b0 + excl;  // segment open before this lane's first nnz
@@ -256,7 +257,7 @@ __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
     const int nwrite = total + (closes ? 1 : 0) - (int)b0;
     __syncwarp();
     for (int i = lane; i < nwrite; i += 32) {
-        double *yp = y + (ne ? __ldg(ne + tseg + i) : tseg + i);
+        double *yp = y + (NE && ne ? __ldg(ne + tseg + i) : tseg + i);
         const double yv = beta == 0.0 ? 0.0 : (i < 32 ? ya : (i < 64 ? yb : ld_y(yp, stream)));
         st_y(yp, y_update(alpha, s_sum[i], beta, yv), stream);
     }
