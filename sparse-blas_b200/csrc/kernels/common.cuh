@@ -127,4 +127,19 @@ __device__ __forceinline__ void write_y(double *yp, double alpha, double sum, do
     st_y(yp, y_update(alpha, sum, beta, beta == 0.0 ? 0.0 : ld_y(yp, pol)), pol);
 }
 
+// Programmatic dependent launch (sm_90+): a kernel launched with the
+// programmatic-serialization attribute may start before the kernel ahead of
+// it in the stream has finished; grid_dependency_wait() blocks until that
+// grid has completed and its memory operations are visible.
+// allow_dependent_launch() lets the next such kernel be scheduled as soon as
+// every block of this grid has executed it (each block's exit counts too).
+__device__ __forceinline__ void grid_dependency_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void allow_dependent_launch()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace sbb

@@ -72,6 +72,9 @@ fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cva
              int n_long, int n_runs_host, int warp_blocks, double alpha, double *__restrict__ y,
              unsigned *queue, const int *dev_count)
 {
+    // Launched as a programmatic dependent of the kernel before it: nothing
+    // is read before that grid has completed and its writes are visible.
+    grid_dependency_wait();
     if (blockIdx.x >= long_blocks && blockIdx.x < long_blocks + warp_blocks) {
         const int j = n_long + (blockIdx.x - long_blocks) * (FT / 32) + (threadIdx.x >> 5);
         if (j >= n_runs_host) return;
@@ -184,9 +187,22 @@ void launch_fixup(int m, const int *crow, const double *cval, int T, const Carry
     if (short_blocks > 148 * 8) short_blocks = 148 * 8;
     const int long_blocks = dev_count ? 148 : R.n_long;
     const int warp_blocks = dev_count ? 0 : (R.n_runs - R.n_long + FT / 32 - 1) / (FT / 32);
-    fixup_kernel<<<short_blocks + long_blocks + warp_blocks, FT, 0, s>>>(
-        m, crow, cval, T, R.run_first, R.run_len, long_blocks, R.n_long, R.n_runs, warp_blocks,
-        alpha, y, queue, dev_count);
+    // Programmatic dependent launch: the fix-up's blocks are placed while the
+    // producing kernel drains and wait in grid_dependency_wait(), which hides
+    // the launch gap between the two kernels.
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(short_blocks + long_blocks + warp_blocks);
+    cfg.blockDim = dim3(FT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, fixup_kernel, m, crow, cval, T, (const int *)R.run_first,
+                       (const int *)R.run_len, long_blocks, R.n_long, R.n_runs, warp_blocks, alpha,
+                       y, queue, dev_count);
 }
 
 }  // namespace sbb

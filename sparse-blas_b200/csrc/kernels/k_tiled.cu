@@ -275,6 +275,9 @@ tiled_kernel(int m, int n, long long nnz, int tiles, const unsigned char *__rest
             if (t + b * W < tiles) issue(t + b * W, b);
     }
     __syncwarp();
+    // The carry fix-up after this kernel is a programmatic dependent launch:
+    // its blocks may take the SM slots this grid frees while it drains.
+    allow_dependent_launch();
 
     unsigned timeout = 0;
     uint32_t phases = 0u;  // bit b: parity of buffer b's next phase
