@@ -47,9 +47,10 @@ int spMV_mgpu_v1(int m, int n, long long nnz, double *alpha, double *csrVal,
 
 /* Replaces spMV_mgpu_v2 (SparseBLAS/include/spmv_kernel.h:21-28,
  * SparseBLAS/src/dspmv_mgpu_v2.cu:33-207).  ceil(nnz/nb) tasks with the
- * reference's split-row merge; the task pool runs as one persistent kernel
- * with q resident CTAs per SM.  Returns 0 on success (the reference returns
- * no value, :207). */
+ * reference's split-row merge.  With kernel 2 the task pool runs as one
+ * persistent merge kernel: q resident CTAs per SM claim items of nb nnz
+ * (capped so every warp gets several) from a device work queue.  Returns 0
+ * on success (the reference returns no value, :207). */
 int spMV_mgpu_v2(int m, int n, long long nnz, double *alpha, double *csrVal,
                  long long *csrRowPtr, int *csrColIndex, double *x,
                  double *beta, double *y, int ngpu, int kernel, long long nb,

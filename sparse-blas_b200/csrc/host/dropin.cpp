@@ -206,7 +206,7 @@ double csrmv_value(double alpha, double sum, double beta, double y0)
 // enough memory, device error), 1 (allocation failure).
 int run(int m, int n, long long nnz, double alpha, const double *val, const long long *rp,
         const int *col, const double *x, double beta, double *y, std::vector<Slice> &sl,
-        Merge merge, int kernel, int q)
+        Merge merge, int kernel, int q, long long queue_nnz = 0)
 {
     // Slices that cover at least one row, and the hull of covered rows.
     int hr0 = INT_MAX, hr1 = -1;
@@ -367,6 +367,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         p.col = d_col;
         p.val = d_val;
         p.status = nullptr;
+        p.queue_nnz = queue_nnz;
         sbb_config cfg{};
         cfg.kernel = kernel;
         cfg.persistent = q;
@@ -550,8 +551,10 @@ int dropin_v2(int m, int n, long long nnz, double *alpha, double *val, long long
     if (nb <= 0) return -1;
     if (m == 0 || nnz == 0) return 0;
     auto sl = v2_slices(m, nnz, rp, y, nb);
+    // The task pool becomes the merge kernel's device work queue: q resident
+    // CTAs per SM claim items of nb nnz (see merge_queue_item for the cap).
     return run(m, n, nnz, *alpha, val, rp, col, x, *beta, y, sl, Merge::V2,
-               kernel == 2 ? SBB_KERNEL_MERGE : kernel, kernel == 2 ? q : 0);
+               kernel == 2 ? SBB_KERNEL_MERGE : kernel, kernel == 2 ? q : 0, nb);
 }
 
 }  // namespace sbb

@@ -302,6 +302,21 @@ int plan_build_unchecked(Plan *p, const sbb_config *cfg, cudaStream_t s)
     return plan_build_impl(p, cfg, s, false);
 }
 
+// Segments a warp of the persistent merge form claims from the work queue at
+// a time: queue_nnz rounded up to whole segments (one segment when unset),
+// but at most a quarter of the segments per warp of the grid, so that every
+// warp still claims several items (an item as large as a reference task,
+// nnz / 8 for example, would leave most of the GPU idle).
+int merge_queue_item(const Plan &p)
+{
+    const long long seg = 32LL * p.ipt;
+    long long item = p.queue_nnz > 0 ? (p.queue_nnz + seg - 1) / seg : 1;
+    const long long warps = (long long)p.persistent_ctas * (kMergeThreads / 32);
+    const long long cap = warps > 0 ? p.tiles / (4 * warps) : 1;
+    item = std::min(item, std::max(cap, 1LL));
+    return (int)std::max(item, 1LL);
+}
+
 int plan_run(Plan *p, double alpha, const void *x, double beta, double *y, cudaStream_t s)
 {
     CsrView A{p->m, p->n, p->rowptr, p->col, p->val};
@@ -317,7 +332,7 @@ int plan_run(Plan *p, double alpha, const void *x, double beta, double *y, cudaS
         break;
     case SBB_KERNEL_MERGE: {
         MergeScratch S{p->tile_row, p->tile_nnz, p->carry_val, &p->runs, nullptr, p->tiles,
-                       p->queue, p->persistent_ctas};
+                       p->queue, p->persistent_ctas, merge_queue_item(*p)};
         if (p->f32)
             launch_merge_f32(A, p->ipt, S, alpha, static_cast<const float *>(x), beta, y,
                              p->status, s);

@@ -69,8 +69,12 @@ __global__ void merge_partition_kernel(const int *__restrict__ rowptr, int m, in
     tile_nnz[p] = z;
 }
 
-// One warp per segment; with `persistent`, a fixed grid whose warps take
-// segments w, w + W, w + 2W, ... (W = warps in the grid).
+// One warp per segment; in the persistent form (queue non-null) a fixed grid
+// whose warps claim `item` consecutive segments at a time from a device work
+// queue (queue[0], an atomicAdd head, zeroed again by the fix-up after the
+// kernel) until the segments run out.  Which warp computes a segment does
+// not change its arithmetic, so results are the same as one warp per
+// segment.
 template <int IPT> struct MergeShape {
     static constexpr int MINB = IPT <= 8 ? 4 : 2;  // CTAs per SM the launch bounds aim at
 };
@@ -81,16 +85,29 @@ merge_kernel(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
              const typename PT::V *__restrict__ val, const typename PT::V *__restrict__ x,
              double *__restrict__ y, double alpha, double beta, const int *__restrict__ tile_row,
              const int *__restrict__ tile_nnz, double *__restrict__ carry_val, int tiles,
-             unsigned *status)
+             unsigned *status, unsigned *queue, int item)
 {
     using P = typename PT::P;
     constexpr int SEG = 32 * IPT;
     __shared__ P s_p[WPB][SEG];
     __shared__ int s_re[WPB][SEG + 1];
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t keep = l2_evict_last(), streaming = l2_evict_first();
-    const int W = gridDim.x * WPB;
-    for (int w = blockIdx.x * WPB + warp; w < tiles; w += W)
+    if (queue) {
+        for (;;) {
+            unsigned first = 0;
+            if (lane == 0) first = atomicAdd(queue, (unsigned)item);
+            first = __shfl_sync(0xffffffffu, first, 0);
+            if (first >= (unsigned)tiles) break;
+            const int end = (int)min((unsigned long long)first + item, (unsigned long long)tiles);
+            for (int w = (int)first; w < end; ++w)
+                merge_segment<PT, ACC, IPT>(w, n, rowptr, col, val, x, y, alpha, beta, tile_row,
+                                            tile_nnz, carry_val, status, s_p[warp], s_re[warp],
+                                            keep, streaming);
+        }
+        return;
+    }
+    for (int w = blockIdx.x * WPB + warp; w < tiles; w += gridDim.x * WPB)
         merge_segment<PT, ACC, IPT>(w, n, rowptr, col, val, x, y, alpha, beta, tile_row,
                                     tile_nnz, carry_val, status, s_p[warp], s_re[warp], keep,
                                     streaming);
@@ -104,15 +121,16 @@ void launch_merge_t(const CsrView &A, const MergeScratch &S, double alpha,
     const auto *val = static_cast<const typename PT::V *>(A.val);
     if (S.tiles > 0) {
         long long blocks = (S.tiles + WPB - 1) / WPB;
-        int grid = (int)(S.persistent_ctas > 0 && S.persistent_ctas < blocks ? S.persistent_ctas
-                                                                             : blocks);
+        const bool queued = S.queue && S.persistent_ctas > 0 && S.persistent_ctas < blocks;
+        int grid = (int)(queued ? S.persistent_ctas : blocks);
         hook_start(s);
         merge_kernel<PT, ACC, IPT><<<grid, NT, 0, s>>>(A.n, A.rowptr, A.col, val, x, y, alpha, beta,
                                                        S.tile_row, S.tile_nnz, S.carry_val,
-                                                       S.tiles, status);
+                                                       S.tiles, status, queued ? S.queue : nullptr,
+                                                       S.queue_item > 0 ? S.queue_item : 1);
         hook_stop(s);
-        launch_fixup(A.m, S.tile_row + 1, S.carry_val, S.tiles, *S.runs, alpha, y, nullptr, s,
-                     S.runs_count);
+        launch_fixup(A.m, S.tile_row + 1, S.carry_val, S.tiles, *S.runs, alpha, y,
+                     queued ? S.queue : nullptr, s, S.runs_count);
     }
 }
 

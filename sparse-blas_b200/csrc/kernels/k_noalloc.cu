@@ -160,7 +160,7 @@ extern "C" int sbb_spmv_merge_noalloc(int m, int n, int nnz, const int *d_rowptr
     CarryRuns runs;
     runs.run_first = run_first;
     runs.run_len = run_len;
-    MergeScratch S{tile_row, tile_nnz, carry_val, &runs, run_count, tiles, nullptr, 0};
+    MergeScratch S{tile_row, tile_nnz, carry_val, &runs, run_count, tiles, nullptr, 0, 1};
     launch_merge(A, kIpt, S, alpha, d_x, beta, d_y, status, s);
     SBB_CUDA(cudaGetLastError());
     return SBB_OK;

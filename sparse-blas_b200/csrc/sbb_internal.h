@@ -142,8 +142,9 @@ struct MergeScratch {
     const CarryRuns *runs;
     const int *runs_count;            // non-null: run count kept on the device
     int tiles;
-    unsigned *queue;                  // persistent form: [0] = next tile, [1] = done
+    unsigned *queue;                  // persistent form: [0] = next segment to claim
     int persistent_ctas;              // 0 = one CTA per tile
+    int queue_item;                   // persistent form: segments per claim (>= 1)
 };
 void launch_merge(const CsrView &A, int ipt, const MergeScratch &S, double alpha,
                   const double *x, double beta, double *y, unsigned *status,
@@ -259,6 +260,7 @@ struct Plan {
     int vector_width = 0;    // K1
     int ipt = 0;             // K2
     int persistent = 0;      // K2 persistent CTAs per SM (0 = off)
+    long long queue_nnz = 0; // K2 persistent form: nnz per queue item (0 = one segment)
     int tile_sigma = 0;      // K3
     int max_row = 0, empty_rows = 0;
     // device scratch owned by the plan

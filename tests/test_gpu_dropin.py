@@ -245,3 +245,26 @@ def test_dropin_large_call_chunked(cuda, version, kernel):
     assert max_scaled_err(yy, y_ref, sc) <= TOL_FP64
     untouched = y_ref == y
     assert np.array_equal(yy[untouched], y[untouched])
+
+
+@pytest.mark.parametrize("nb_div,q", [(400, 1), (400, 4), (3, 2), (1, 8)])
+def test_v2_task_queue_matches_oracle(cuda, nb_div, q):
+    """spMV_mgpu_v2 with kernel 2: the tasks run as the merge kernel's device
+    work queue (q CTAs per SM, items of nb nnz up to the cap); every nb and q
+    gives the oracle driver's result, and a repeated call the same bits."""
+    from sbb import api
+    rp, col, val, x, y = rand_csr(12, 150000, 120000, 0, 24)
+    m, n, nnz = len(rp) - 1, len(x), int(rp[-1])
+    nb = max(1, nnz // nb_div)
+    rc_ref, y_ref = O.dropin("v2", m, n, nnz, 1.3, val, rp, col, x, -0.6, y, ngpu=1, kernel=2,
+                             nb=nb, q=q)
+    assert rc_ref == 0
+    _, sc = O.spmv_dd(rp, col, val, x, 1.3, -0.6, y)
+    outs = []
+    for _ in range(2):
+        yy = y.copy()
+        assert api.spMV_mgpu_v2(m, n, nnz, 1.3, val, rp, col, x, -0.6, yy, ngpu=1, kernel=2,
+                                nb=nb, q=q) == 0
+        outs.append(yy)
+    assert max_scaled_err(outs[0], y_ref, sc) <= TOL_FP64
+    assert np.array_equal(outs[0], outs[1])

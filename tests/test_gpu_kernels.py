@@ -489,3 +489,37 @@ def test_plan_spmv_captured_in_cuda_graph(cuda, cfg):
     assert torch.equal(y_graph, y_direct)
     del g
     P.close()
+
+
+@pytest.mark.parametrize("persistent", [1, 2, 4])
+def test_merge_work_queue_same_bits(cuda, persistent):
+    """The persistent merge form, whose warps claim segments from a device
+    work queue, gives the same bits as one warp per segment, call after call
+    (the fix-up re-arms the queue), directly and from a CUDA graph."""
+    import torch
+    from sbb.device import Plan
+    rp, col, val, x, y = rand_csr(11, 200000, 150000, 0, 20, long_rows=[(7, 90000)])
+    drp, dcol, dval, dx, dy = to_dev(rp, col, val, x, y)
+    ref, _ = run_plan(rp, col, val, x, y, len(x), 0.9, 0.4, dict(kernel="merge", items_per_thread=8))
+    P = Plan(drp, dcol, dval, len(x), kernel="merge", items_per_thread=8, persistent=persistent)
+    info = P.info()
+    assert 0 < info["persistent"] and info["persistent"] * 8 < info["tiles"]  # the queue is used
+    for _ in range(3):
+        yy = dy.clone()
+        P.spmv(dx, yy, 0.9, 0.4)
+        torch.cuda.synchronize()
+        assert np.array_equal(yy.cpu().numpy(), ref[0])
+    yg = dy.clone()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=torch.cuda.Stream()):
+        P.spmv(dx, yg, 0.9, 0.4)
+    for _ in range(2):
+        yg.copy_(dy)
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(yg.cpu().numpy(), ref[0])
+    del g
+    P.check()
+    P.close()
+    y_ref, sc = O.spmv_dd(rp, col, val, x, 0.9, 0.4, y)
+    assert max_scaled_err(ref[0], y_ref, sc) <= TOL_FP64
