@@ -211,21 +211,39 @@ def single_thread(A, x, y, alpha, beta, args):
 
 
 def run_reference(args, ws, rank):
+    """The reference's host CSR loop on all host cores: W warm-up passes and
+    K timed passes over the same matrix as the GPU arm (each step one full
+    SpMV), the timed passes stopped early only past two minutes."""
     if rank != 0:
         return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
     A, x, y, alpha, beta, desc = make_workload(args.workload)
     threads = os.cpu_count() or 1
-    sec, reps = cpu_sample_time(A, x, y, alpha, beta, threads, budget_s=args.cpu_budget)
+    rp = np.ascontiguousarray(A.rowptr)
+    for _ in range(max(args.warmup, 1)):
+        O.spmv_host(rp, A.col, A.val, x, alpha, beta, y, threads)
+    steps, t_total = 0, 0.0
+    while steps < max(args.steps, 1) and t_total < 120.0:
+        t0 = time.perf_counter()
+        O.spmv_host(rp, A.col, A.val, x, alpha, beta, y, threads)
+        t_total += time.perf_counter() - t0
+        steps += 1
+    sec = t_total / steps
     gbs = algo_bytes(A.m, A.n, A.nnz) / sec / 1e9
     one = single_thread(A, x, y, alpha, beta, args)
     line = {
         "metric": "SpMV HBM GB/s (FP64 CSR, algorithmic bytes 12*nnz+4*(m+1)+8*n+16*m)",
         "value": round(gbs, 3), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
-        "steps": reps, "warmup": 1, "ms_per_step": round(sec * 1e3, 3),
+        "steps": steps, "warmup": max(args.warmup, 1), "ms_per_step": round(sec * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": desc, "nnz": A.nnz, "threads": threads},
+        "data": "synthetic",
+        "GFLOP/s": round((2 * A.nnz + 3 * A.m) / sec / 1e9, 2),
+        "config": {"workload": desc, "m": A.m, "n": A.n, "nnz": A.nnz,
+                   "kernel": "host CSR loop (main.cu:350-356)", "threads": threads,
+                   "parallelism": f"replicas x{args.gpus}"},
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"{reps} full passes of the host CSR loop (main.cu:350-356 "
+                         "sample": f"{steps} full passes of the host CSR loop (main.cu:350-356 "
                                    f"restated with +beta*y, OpenMP static over rows)",
                          "single_thread": one},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
@@ -898,6 +916,8 @@ def run_sbb(args, ws, rank, local):
                                                 "vector_width", "tiles")},
                        "l2": "inputs larger than L2 (working set %.0f MB), no flush" % (bytes_step / 1e6),
                        "parallelism": f"replicas x{ws}"},
+            "GFLOP/s": round(ws * (2 * nnz + 3 * m) / (ms_step * 1e-3) / 1e9, 2),
+            "kernel_GFLOP/s": round((2 * nnz + 3 * m) / (kern_avg * 1e-3) / 1e9, 2),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "peak_source": peak_kind,
