@@ -36,7 +36,9 @@ static_assert(TBB % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // Per class kernel: dynamic shared memory per warp (merge: a segment's
 // staging; tiled: two unit slots) and the CTAs per SM its register budget
-// aims at (no spills at any of them).
+// aims at.  The vector families spill a few dozen bytes at 64 registers;
+// at 3 CTAs per SM they do not, but the 512-matrix batch ran slower (4.85
+// vs 4.73 ms).
 template <int FAM> struct FamShape {  // vector families
     static constexpr size_t kWarpBytes = 0;
     static constexpr int MINB = 4;
