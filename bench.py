@@ -815,35 +815,63 @@ def run_sbb(args, ws, rank, local):
             yp[:] = y_h
             assert api.spMV_mgpu_v1(m, n, nnz, alpha, valp, rp64, colp, xp, beta, yp, 1, 2) == 0
         e_steps = max(3, min(args.steps, 10))
-        barrier(ws)
-        torch.cuda.synchronize()
-        tt = time.perf_counter()
-        for _ in range(e_steps):
-            rc = api.spMV_mgpu_v1(m, n, nnz, alpha, valp, rp64, colp, xp, beta, yp, 1, 2)
-            assert rc == 0
-        e_sec = (time.perf_counter() - tt) / e_steps
-        e_sec = max_over_ranks(e_sec, ws)
         h2d = 8 * (m + 1) + 4 * nnz + 8 * nnz + 8 * n + (8 * m if beta != 0 else 0)
         # This box's PCIe floor: the same bytes as plain pinned copies (host
-        # to device, then y back), timed the same way.
+        # to device, then y back), timed after each call so that both see the
+        # same moment of the host's and the link's other traffic.
         src = [pinned[id(a)] for a in (rp64, colp, valp, xp) + ((yp,) if beta != 0 else ())]
         dst = [torch.empty_like(t_, device=dev) for t_ in src]
         yback = pinned[id(yp)]
-        ydev = torch.empty_like(yback, device=dev)
+        ydev = torch.zeros_like(yback, device=dev)
+        call_s, copy_s, phases = [], [], []
+        ph = (C.c_double * 5)()
         barrier(ws)
         torch.cuda.synchronize()
-        tt = time.perf_counter()
         for _ in range(e_steps):
+            tt = time.perf_counter()
+            rc = api.spMV_mgpu_v1(m, n, nnz, alpha, valp, rp64, colp, xp, beta, yp, 1, 2)
+            call_s.append(time.perf_counter() - tt)
+            assert rc == 0
+            if lib().sbb_last_call_phases(ph, 5) == 5:
+                phases.append(list(ph))
+            tt = time.perf_counter()
             for d_, s_ in zip(dst, src):
                 d_.copy_(s_, non_blocking=True)
             yback.copy_(ydev, non_blocking=True)
             torch.cuda.synchronize()
-        c_sec = max_over_ranks((time.perf_counter() - tt) / e_steps, ws)
+            copy_s.append(time.perf_counter() - tt)
+        # The same copies with y going back on a second stream while the
+        # matrix goes in (both directions of the link at once, as the call's
+        # chunked pipeline does).
+        both_s = []
+        side = torch.cuda.Stream()
+        for _ in range(e_steps):
+            torch.cuda.synchronize()
+            tt = time.perf_counter()
+            with torch.cuda.stream(side):
+                yback.copy_(ydev, non_blocking=True)
+            for d_, s_ in zip(dst, src):
+                d_.copy_(s_, non_blocking=True)
+            torch.cuda.synchronize()
+            both_s.append(time.perf_counter() - tt)
+        yp[:] = y_h  # the floor's copy back overwrote the host y
+        e_sec = max_over_ranks(sum(call_s) / e_steps, ws)
+        c_sec = max_over_ranks(sum(copy_s) / e_steps, ws)
         del dst, ydev
+        spread = lambda v: {"min": round(min(v) * 1e3, 3),  # noqa: E731
+                            "median": round(statistics.median(v) * 1e3, 3),
+                            "max": round(max(v) * 1e3, 3)}
         e2e = {"value": round(ws * bytes_step / e_sec / 1e9, 3), "unit": "GB/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * m,
                "ms_per_step": round(e_sec * 1e3, 3),
                "pcie_copy_floor_ms": round(c_sec * 1e3, 3),
+               "call_ms": spread(call_s), "pcie_copy_floor_call_ms": spread(copy_s),
+               "pcie_copy_both_directions_ms": spread(both_s),
+               "call_phases_ms_median": (dict(zip(
+                   ("host_prep", "rowptr_check_wait", "plans_and_launches", "kernels_and_copy_back",
+                    "host_merges"),
+                   [round(statistics.median(p_[i] for p_ in phases), 3) for i in range(5)]))
+                   if phases else None),
                "api": "spMV_mgpu_v1(kernel=2) host pointers, pinned",
                "note": "the host-pointer call copies the whole matrix, x and y over PCIe in "
                        "every step (most of the step), so it runs the merge-path kernel "

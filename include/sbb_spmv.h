@@ -289,6 +289,18 @@ void sbb_mm_free(void *handle);
 
 const char *sbb_last_error(void);
 
+/* ---- call trace ------------------------------------------------------------ */
+
+/* Wall-clock phases of the calling thread's last host-pointer call
+ * (spMV_mgpu_baseline / v1 / v2), in milliseconds, for finding where a slow
+ * call spends its time: [0] host partition and copy enqueue, [1] wait for
+ * the row-pointer check on the device, [2] plan building and launches of
+ * every chunk, [3] wait for the kernels and the copy of y back, [4] host
+ * merges and restores.  Writes min(n, SBB_TRACE_PHASES) values and returns
+ * how many; 0 if the thread has made no call that got that far. */
+#define SBB_TRACE_PHASES 5
+int sbb_last_call_phases(double *ms, int n);
+
 /* ---- test hooks ------------------------------------------------------------ */
 
 /* Host-side fault injection for the library's own tests, so that the error

@@ -18,6 +18,7 @@
 #include <sys/time.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -126,6 +127,28 @@ enum class Merge { V1, V2, NONE };
 // Per-thread state of the drop-in calls: two streams per device and a few
 // pinned status words, released when the thread ends (so callers that start
 // a thread per call do not accumulate streams or pinned pages).
+// Wall-clock marks of the calling thread's current host-pointer call; the
+// phases between them are published when the call completes
+// (sbb_last_call_phases).
+struct CallTrace {
+    std::chrono::steady_clock::time_point mark[SBB_TRACE_PHASES + 1];
+    double ms[SBB_TRACE_PHASES] = {};
+    int done = 0;  // phases of the last completed call
+};
+thread_local CallTrace g_trace;
+
+void trace_mark(int k)
+{
+    g_trace.mark[k] = std::chrono::steady_clock::now();
+    if (k == SBB_TRACE_PHASES) {
+        for (int i = 0; i < SBB_TRACE_PHASES; ++i)
+            g_trace.ms[i] =
+                std::chrono::duration<double, std::milli>(g_trace.mark[i + 1] - g_trace.mark[i])
+                    .count();
+        g_trace.done = SBB_TRACE_PHASES;
+    }
+}
+
 struct ThreadState {
     cudaStream_t s[2][64] = {};
     bool pool_set[64] = {};
@@ -216,6 +239,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
             hr1 = std::max(hr1, t.end_row);
         }
     if (hr1 < 0) return 0;  // nothing covered (e.g. nnz == 0 with a tie)
+    trace_mark(0);
 
     // Special rows: slice extent != CSR extent, or split.
     std::vector<Piece> pieces;
@@ -340,7 +364,9 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
                                cudaMemcpyHostToDevice, s));
         ck(cudaEventRecord(ev_copy[k], s));
     }
+    trace_mark(1);
     ck(cudaEventSynchronize(ev));
+    trace_mark(2);
     cudaEventDestroy(ev);
     const unsigned h_st = h_pin[0];
     if (!cuda_ok || (h_st & ST_BAD_ROWPTR)) {
@@ -419,7 +445,9 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
     ck(cudaMemcpyAsync(pst + kChunks, d_st, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     ck(cudaEventRecord(ev_done, s2));
     ck(cudaStreamWaitEvent(s, ev_done, 0));  // the frees below follow every chunk
+    trace_mark(3);
     ck(cudaStreamSynchronize(s));
+    trace_mark(4);
     ck(cudaGetLastError());
     for (auto &p : plans) plan_free_async(&p, s);
     destroy_events();
@@ -490,6 +518,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
             }
         }
     }
+    trace_mark(SBB_TRACE_PHASES);
     return 0;
 }
 
@@ -561,6 +590,14 @@ int dropin_v2(int m, int n, long long nnz, double *alpha, double *val, long long
 
 // ------------------------------------------------------------- C ABI
 extern "C" {
+
+int sbb_last_call_phases(double *ms, int n)
+{
+    const sbb::CallTrace &t = sbb::g_trace;
+    const int k = ms && n > 0 ? std::min(n, t.done) : 0;
+    for (int i = 0; i < k; ++i) ms[i] = t.ms[i];
+    return k;
+}
 
 int spMV_mgpu_baseline(int m, int n, long long nnz, double *alpha, double *csrVal,
                        long long *csrRowPtr, int *csrColIndex, double *x, double *beta,

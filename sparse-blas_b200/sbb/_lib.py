@@ -98,6 +98,7 @@ SIGNATURES = {
     "sbb_spmv_merge_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_double, vp,
                                          C.c_double, vp, vp]),
     "sbb_last_error": (C.c_char_p, []),
+    "sbb_last_call_phases": (C.c_int, [dp, C.c_int]),
     "sbb_test_hook": (C.c_int, [C.c_int, C.c_longlong]),
 }
 

@@ -268,3 +268,33 @@ def test_v2_task_queue_matches_oracle(cuda, nb_div, q):
         outs.append(yy)
     assert max_scaled_err(outs[0], y_ref, sc) <= TOL_FP64
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_last_call_phases(cuda):
+    """sbb_last_call_phases: nothing before a thread's first call, then five
+    non-negative phases of the last call that add up to at most its wall
+    time."""
+    import ctypes as C
+    import threading
+    import time
+    from sbb import api
+    from sbb._lib import lib
+    got = {}
+
+    def worker():
+        ph = (C.c_double * 5)()
+        got["before"] = lib().sbb_last_call_phases(ph, 5)
+        rp, col, val, x, y = rand_csr(13, 3000, 2500, 0, 16)
+        m, n, nnz = len(rp) - 1, len(x), int(rp[-1])
+        t0 = time.perf_counter()
+        got["rc"] = api.spMV_mgpu_v1(m, n, nnz, 1.0, val, rp, col, x, 0.5, y.copy(), ngpu=1, kernel=2)
+        got["wall_ms"] = (time.perf_counter() - t0) * 1e3
+        got["n"] = lib().sbb_last_call_phases(ph, 5)
+        got["ph"] = list(ph)
+        got["n2"] = lib().sbb_last_call_phases(ph, 2)
+
+    th = threading.Thread(target=worker)
+    th.start()
+    th.join()
+    assert got["before"] == 0 and got["rc"] == 0 and got["n"] == 5 and got["n2"] == 2
+    assert all(v >= 0.0 for v in got["ph"]) and sum(got["ph"]) <= got["wall_ms"] + 1e-6
