@@ -658,6 +658,7 @@ def config_line(name, kernel, kw, local, cpu_budget, reps=200):
                            if r["graph_step_ms"] else None),
             "GB/s": round(b / (r["step_ms"] * 1e-3) / 1e9, 2),
             "GFLOP/s": round(fl / (r["step_ms"] * 1e-3) / 1e9, 2),
+            "traffic": traffic_from_profile(tag, name),
             "kernel_GB/s": round(b / (r["kernel_ms"] * 1e-3) / 1e9, 2),
             "frac": round(b / (r["kernel_ms"] * 1e-3) / 1e9 / peak, 4), "peak": peak,
             "peak_source": peak_kind, "algorithmic_bytes": b, "flops": fl,
