@@ -394,6 +394,7 @@ int run(int m, int n, long long nnz, double alpha, const double *val, const long
         p.val = d_val;
         p.status = nullptr;
         p.queue_nnz = queue_nnz;
+        p.device_runs = true;  // no host synchronisation while the copies stream in
         sbb_config cfg{};
         cfg.kernel = kernel;
         cfg.persistent = q;

@@ -247,7 +247,10 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
         if (tiles > 0) {
             launch_merge_partition(p->rowptr, p->m, p->base, p->nnz, items, p->tiles, p->tile_row,
                                    p->tile_nnz, s);
-            if ((rc = carry_runs_build(p->tile_row + 1, p->tiles, p->m, &p->runs, s))) return rc;
+            rc = p->device_runs
+                     ? carry_runs_build_device(p->tile_row + 1, p->tiles, p->m, &p->runs, s)
+                     : carry_runs_build(p->tile_row + 1, p->tiles, p->m, &p->runs, s);
+            if (rc) return rc;
             p->scratch_bytes += p->runs.bytes;
         }
         if (p->persistent > 0) {
@@ -331,7 +334,7 @@ int plan_run(Plan *p, double alpha, const void *x, double beta, double *y, cudaS
                           p->status, s);
         break;
     case SBB_KERNEL_MERGE: {
-        MergeScratch S{p->tile_row, p->tile_nnz, p->carry_val, &p->runs, nullptr, p->tiles,
+        MergeScratch S{p->tile_row, p->tile_nnz, p->carry_val, &p->runs, p->runs.count, p->tiles,
                        p->queue, p->persistent_ctas, merge_queue_item(*p)};
         if (p->f32)
             launch_merge_f32(A, p->ipt, S, alpha, static_cast<const float *>(x), beta, y,

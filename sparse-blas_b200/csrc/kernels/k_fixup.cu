@@ -96,10 +96,22 @@ fixup_kernel(int m, const int *__restrict__ crow, const double *__restrict__ cva
         return;
     }
     __shared__ double s[FT];
-    // with a device-side count, a fixed set of blocks strides over the runs
+    // With a device-side count, a fixed set of blocks goes over all the runs
+    // twice: every warp takes runs of at most kWarpRunMax carries (the same
+    // warp sum as above), then every block the longer ones.
+    if (dev_count) {
+        const int n_all = *dev_count, nw = long_blocks * (FT / 32);
+        for (int j = blockIdx.x * (FT / 32) + (threadIdx.x >> 5); j < n_all; j += nw) {
+            const int first = run_first[j], len = run_len[j];
+            if (len > kWarpRunMax) continue;
+            const double sum = fixup_run_warp(cval, first, len);
+            if ((threadIdx.x & 31) == 0) fixup_single(y, crow[first], alpha, sum);
+        }
+    }
     const int n_runs = dev_count ? *dev_count : n_long;
     for (int j = blockIdx.x; j < n_runs; j += long_blocks) {
         const int first = run_first[j], len = run_len[j];
+        if (dev_count && len <= kWarpRunMax) continue;  // block-uniform: summed above
         s[threadIdx.x] = fixup_partial(cval, first, len, threadIdx.x);
         __syncthreads();
         for (int w = FT / 2; w > 0; w >>= 1) {
@@ -157,15 +169,36 @@ int carry_runs_build(const int *crow, int T, int m, CarryRuns *R, cudaStream_t s
     return SBB_OK;
 }
 
+int carry_runs_build_device(const int *crow, int T, int m, CarryRuns *R, cudaStream_t s)
+{
+    R->n_runs = 0;
+    R->n_long = 0;
+    R->run_first = R->run_len = R->count = nullptr;
+    if (T <= 0) return SBB_OK;
+    const int cap = T / 2 + 1;
+    if (dev_malloc_async((void **)&R->run_first, sizeof(int) * cap, s) != cudaSuccess ||
+        dev_malloc_async((void **)&R->run_len, sizeof(int) * cap, s) != cudaSuccess ||
+        dev_malloc_async((void **)&R->count, sizeof(int), s) != cudaSuccess) {
+        set_error("carry runs: device allocation failed");
+        return SBB_ERR_NOMEM;
+    }
+    R->bytes = 2 * sizeof(int) * (size_t)cap + sizeof(int);
+    SBB_CUDA(cudaMemsetAsync(R->count, 0, sizeof(int), s));
+    runs_mark_kernel<<<(T + FT - 1) / FT, FT, 0, s>>>(crow, T, m, R->run_first, R->run_len,
+                                                      R->count);
+    return SBB_OK;
+}
+
 void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async)
 {
-    for (int *p : {R->run_first, R->run_len})
+    for (int *p : {R->run_first, R->run_len, R->count})
         if (p) {
             if (async)
                 cudaFreeAsync(p, s);
             else
                 cudaFree(p);
         }
+    R->count = nullptr;
     R->run_first = R->run_len = nullptr;
     R->n_runs = 0;
     R->n_long = 0;

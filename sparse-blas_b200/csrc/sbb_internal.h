@@ -118,9 +118,13 @@ struct CarryRuns {
     int *run_first = nullptr, *run_len = nullptr;
     int n_runs = 0;
     int n_long = 0;   // runs longer than kWarpRunMax, listed first
+    int *count = nullptr;  // device-built lists: the run count, on the device only
     size_t bytes = 0;
 };
 int carry_runs_build(const int *carry_row, int T, int m, CarryRuns *R, cudaStream_t s);
+// The same lists built without any host synchronisation: runs in the order
+// the marking kernel found them, their count left on the device (R->count).
+int carry_runs_build_device(const int *carry_row, int T, int m, CarryRuns *R, cudaStream_t s);
 void carry_runs_free(CarryRuns *R, cudaStream_t s, bool async);
 // Marks the runs on the device only; the count stays in *dev_count.
 void launch_runs_mark(const int *carry_row, int T, int m, int *run_first, int *run_len,
@@ -260,6 +264,7 @@ struct Plan {
     int vector_width = 0;    // K1
     int ipt = 0;             // K2
     int persistent = 0;      // K2 persistent CTAs per SM (0 = off)
+    bool device_runs = false; // K2: carry runs built and counted on the device (no host sync)
     long long queue_nnz = 0; // K2 persistent form: nnz per queue item (0 = one segment)
     int tile_sigma = 0;      // K3
     int max_row = 0, empty_rows = 0;

@@ -298,3 +298,26 @@ def test_last_call_phases(cuda):
     th.join()
     assert got["before"] == 0 and got["rc"] == 0 and got["n"] == 5 and got["n2"] == 2
     assert all(v >= 0.0 for v in got["ph"]) and sum(got["ph"]) <= got["wall_ms"] + 1e-6
+
+
+def test_v1_merge_same_bits_as_merge_plan(cuda):
+    """A host-pointer call with kernel 2 builds its carry runs on the device
+    (no host synchronisation) and still sums every run as the plan API's
+    merge plan does: warp sums for runs of at most 1,024 carries, block trees
+    for longer ones, so y is the same bit for bit."""
+    import torch
+    from sbb import api
+    from sbb.device import Plan
+    rp, col, val, x, y = rand_csr(14, 3000, 300000, 0, 8, long_rows=[(5, 220000), (77, 20000)])
+    m, n, nnz = len(rp) - 1, len(x), int(rp[-1])
+    yy = y.copy()
+    assert api.spMV_mgpu_v1(m, n, nnz, 0.8, val, rp, col, x, 0.3, yy, ngpu=1, kernel=2) == 0
+    d = torch.device("cuda:0")
+    P = Plan(torch.from_numpy(rp.astype(np.int32)).to(d), torch.from_numpy(col).to(d),
+             torch.from_numpy(val).to(d), n, kernel="merge")
+    yd = torch.from_numpy(y).to(d)
+    P.spmv(torch.from_numpy(x).to(d), yd, 0.8, 0.3)
+    torch.cuda.synchronize()
+    P.check()
+    P.close()
+    assert np.array_equal(yy, yd.cpu().numpy())
