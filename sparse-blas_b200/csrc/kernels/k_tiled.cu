@@ -70,22 +70,31 @@ __device__ __forceinline__ long long slot2(int g, int lane, int j)
     return g * 128 + (j >> 1) * 64 + lane * 2 + (j & 1);
 }
 
+// One thread per tile slot, in original nnz order: the column and value of
+// the slot (zeros past nnz), and for the first slots of each tile a zero
+// word of its row-start bits and header, which the later plan kernels OR
+// into and write.  Sigma and the value width are compile-time, so the slot
+// arithmetic is shifts and masks.
+template <int SIGMA, int VB>
 __global__ void blob_fill_kernel(const int *__restrict__ rp, const int *__restrict__ col,
-                                 const void *__restrict__ val, int vbytes, long long nnz, int n,
-                                 int sigma, int tiles, unsigned char *__restrict__ blob,
-                                 unsigned *status)
+                                 const void *__restrict__ val, long long nnz, int n, int tiles,
+                                 unsigned char *__restrict__ blob, unsigned *status)
 {
+    constexpr long long TILE = 32LL * SIGMA;
+    constexpr size_t TB = tile_bytes_of(SIGMA, VB);
+    constexpr size_t DATA = (size_t)TILE * (4 + VB);
+    constexpr int META_WORDS = (int)((TB - DATA) / 4);  // row-start bits and header
+    static_assert((TB - DATA) % 4 == 0 && META_WORDS <= TILE, "tile layout");
     bool bad = false;
-    const long long TILE = 32LL * sigma;
-    const size_t TB = tile_bytes_of(sigma, vbytes);
     const long long first = rp[0];  // the view's nnz start at rowptr[0]
     const long long total = (long long)tiles * TILE;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         // e enumerates (tile, lane, group, j) in original nnz order
-        long long t = e / TILE, q = e % TILE;
-        int lane = (int)(q / sigma), s = (int)(q % sigma), g = s >> 2, j = s & 3;
-        bool in = e < nnz;
+        const long long t = e / TILE;
+        const int q = (int)(e % TILE);
+        const int lane = q / SIGMA, sl = q % SIGMA, g = sl >> 2, j = sl & 3;
+        const bool in = e < nnz;
         unsigned char *tb = blob + (size_t)t * TB;
         int c = in ? col[first + e] : 0;
         if ((unsigned)c >= (unsigned)n) {  // checked once here: the kernel trusts the copy
@@ -93,14 +102,31 @@ __global__ void blob_fill_kernel(const int *__restrict__ rp, const int *__restri
             c = 0;
         }
         reinterpret_cast<int *>(tb)[slot4(g, lane, j)] = c;
-        if (vbytes == 8)
+        if (VB == 8)
             reinterpret_cast<double *>(tb + TILE * 4)[slot2(g, lane, j)] =
                 in ? static_cast<const double *>(val)[first + e] : 0.0;
         else
             reinterpret_cast<float *>(tb + TILE * 4)[slot4(g, lane, j)] =
                 in ? static_cast<const float *>(val)[first + e] : 0.f;
+        if (q < META_WORDS) reinterpret_cast<unsigned *>(tb + DATA)[q] = 0u;
     }
     if (bad) atomicOr(status, ST_BAD_COL);
+}
+
+int grid_for(long long work, int tpb);
+
+template <int VB>
+void launch_blob_fill(int sigma, const int *rp, const int *col, const void *val, long long nnz,
+                      int n, int tiles, unsigned char *blob, unsigned *status, cudaStream_t s)
+{
+    const int grid = grid_for((long long)tiles * 32 * sigma, 256);
+    switch (sigma) {
+    case 4: blob_fill_kernel<4, VB><<<grid, 256, 0, s>>>(rp, col, val, nnz, n, tiles, blob, status); break;
+    case 8: blob_fill_kernel<8, VB><<<grid, 256, 0, s>>>(rp, col, val, nnz, n, tiles, blob, status); break;
+    case 16: blob_fill_kernel<16, VB><<<grid, 256, 0, s>>>(rp, col, val, nnz, n, tiles, blob, status); break;
+    case 32: blob_fill_kernel<32, VB><<<grid, 256, 0, s>>>(rp, col, val, nnz, n, tiles, blob, status); break;
+    default: break;
+    }
 }
 
 // Row-start bits (one per nnz, original order within the tile) and
@@ -477,12 +503,13 @@ int tiled_build(Plan *p, cudaStream_t s)
         set_error("tiled plan: device allocation failed");
         return SBB_ERR_NOMEM;
     }
-    if (tiles > 0) {
-        // bitmaps are OR-ed into zeroed words; cols/vals are then written over
-        SBB_CUDA(cudaMemsetAsync(T->blob, 0, T->tile_bytes * (size_t)tiles, s));
-        blob_fill_kernel<<<grid_for(tiles * TILE, 256), 256, 0, s>>>(
-            p->rowptr, p->col, p->val, vbytes, p->nnz, p->n, T->sigma, T->tiles, T->blob,
-            p->status);
+    if (tiles > 0) {  // every byte of the blob: slots here, bits and headers zeroed here too
+        if (vbytes == 8)
+            launch_blob_fill<8>(T->sigma, p->rowptr, p->col, p->val, p->nnz, p->n, T->tiles,
+                                T->blob, p->status, s);
+        else
+            launch_blob_fill<4>(T->sigma, p->rowptr, p->col, p->val, p->nnz, p->n, T->tiles,
+                                T->blob, p->status, s);
     }
     if (m > 0)
         starts_kernel<<<grid_for(m, 256), 256, 0, s>>>(p->rowptr, m, T->sigma, vbytes, T->blob, flag);
