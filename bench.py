@@ -414,12 +414,13 @@ def run_reference_batch(args, ws, rank):
 
 
 def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local, kernel64=None,
-                kw64=None):
+                kw64=None, lanes=True):
     """FP32-storage compensated form vs the FP64 plan on the same matrix, both
     timed here (main kernel with CUDA events, whole steps), with max and
     median per-row error against the FP64 double-double oracle.  kernel / kw
     configure the FP32 plan, kernel64 / kw64 the FP64 one (default: the
-    same)."""
+    same).  lanes: also the FP32-storage form with FP32 lane sums
+    (sbb_plan_create_f32_lanes, 32 x 8 tiles), keys ``*_lanes``."""
     kernel64 = kernel if kernel64 is None else kernel64
     kw64 = kw if kw64 is None else kw64
     import ctypes as C
@@ -465,21 +466,32 @@ def f32_measure(A, x_h, y_h, alpha, beta, kernel, kw, warmup, steps, local, kern
 
     step64, kern64 = timed(P64, x64)
     step32, kern32 = timed(P32, x32)
-    y = y0.clone()
-    P32.spmv(x32, y, alpha, beta)
-    torch.cuda.synchronize()
-    got = y.cpu().numpy()
     ref, sc = O.spmv_dd(A.rowptr, A.col, A.val, x_h, alpha, beta, y_h)
-    err = np.abs(got - ref) / np.where(sc > 0, sc, 1.0)
+
+    def errors(P):
+        y = y0.clone()
+        P.spmv(x32, y, alpha, beta)
+        torch.cuda.synchronize()
+        err = np.abs(y.cpu().numpy() - ref) / np.where(sc > 0, sc, 1.0)
+        return float(err.max()), float(np.median(err))
+
+    err_max, err_median = errors(P32)
     info = P32.info()
     info64 = P64.info()
     launches = lib().sbb_plan_launches(P32.h)
+    out = dict(step64=step64, kern64=kern64, step32=step32, kern32=kern32,
+               err_max=err_max, err_median=err_median, info=info,
+               info64=info64, launches=launches,
+               tag=KERNEL_TAGS[info["kernel"]], tag64=KERNEL_TAGS[info64["kernel"]])
+    if lanes:
+        PL = Plan(rp, col, P32._keep[2], n, kernel="auto", f32=True, f32_lanes=True)
+        out["step_lanes"], out["kern_lanes"] = timed(PL, x32)
+        out["err_max_lanes"], out["err_median_lanes"] = errors(PL)
+        out["sigma_lanes"] = PL.info()["tile_sigma"]
+        PL.close()
     P64.close()
     P32.close()
-    return dict(step64=step64, kern64=kern64, step32=step32, kern32=kern32,
-                err_max=float(err.max()), err_median=float(np.median(err)), info=info,
-                info64=info64, launches=launches,
-                tag=KERNEL_TAGS[info["kernel"]], tag64=KERNEL_TAGS[info64["kernel"]])
+    return out
 
 
 def run_f32(args, ws, rank, local):
@@ -520,7 +532,8 @@ def run_f32(args, ws, rank, local):
                        "byte_ratio": round(bytes64 / bytes32, 3),
                        "err_max": r["err_max"], "err_median": r["err_median"],
                        "err_metric": "|y - y_oracle| / (|alpha| sum|a x| + |beta y|), FP64 "
-                                     "double-double oracle on the FP64 inputs"},
+                                     "double-double oracle on the FP64 inputs",
+                       "lanes": lanes_keys(r, bytes32, A)},
             "roofline": {"bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 4), "traffic": None, "peak_source": peak_kind},
             "gpu_launches": r["launches"] * args.steps,
@@ -668,6 +681,18 @@ def config_line(name, kernel, kw, local, cpu_budget, reps=200):
                               "sample": f"{cpu_reps} full passes"}}
 
 
+def lanes_keys(r, b32, A):
+    """The FP32-lane-sum form's figures from f32_measure."""
+    return {"api": "sbb_plan_create_f32_lanes", "tile_sigma": r["sigma_lanes"],
+            "kernel_ms": round(r["kern_lanes"], 5), "step_ms": round(r["step_lanes"], 5),
+            "speedup_kernel_vs_fp64": round(r["kern64"] / r["kern_lanes"], 3),
+            "speedup_step_vs_fp64": round(r["step64"] / r["step_lanes"], 3),
+            "GB/s": round(b32 / (r["step_lanes"] * 1e-3) / 1e9, 2),
+            "kernel_GB/s": round(b32 / (r["kern_lanes"] * 1e-3) / 1e9, 2),
+            "GFLOP/s": round((2 * A.nnz + 3 * A.m) / (r["step_lanes"] * 1e-3) / 1e9, 2),
+            "err_max": r["err_max_lanes"], "err_median": r["err_median_lanes"]}
+
+
 def extra_configs(A2, x2, y2, local, cpu_budget):
     """The other benchmark configurations, measured after the timed region of
     the default line (one GPU): c1 and c3 plain, the FP32-storage form on the
@@ -694,7 +719,8 @@ def extra_configs(A2, x2, y2, local, cpu_budget):
                    "f32_GB/s": round(b32 / (r["step32"] * 1e-3) / 1e9, 2),
                    "f32_GFLOP/s": round((2 * A.nnz + 3 * A.m) / (r["step32"] * 1e-3) / 1e9, 2),
                    "byte_ratio": round(b64 / b32, 3),
-                   "err_max": r["err_max"], "err_median": r["err_median"]}
+                   "err_max": r["err_max"], "err_median": r["err_median"],
+                   "lanes": lanes_keys(r, b32, A)}
     f["err_metric"] = ("|y - y_oracle| / (|alpha| sum|a x| + |beta y|) against the FP64 "
                        "double-double oracle on the FP64 inputs")
     out["f32"] = f

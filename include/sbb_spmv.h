@@ -137,6 +137,17 @@ int sbb_plan_create(sbb_plan_t *plan, int m, int n, int nnz,
 int sbb_plan_create_f32(sbb_plan_t *plan, int m, int n, int nnz,
                         const int *d_rowptr, const int *d_col,
                         const float *d_val, const sbb_config *cfg, void *stream);
+/* FP32-storage form with FP32 lane sums: the same storage, but each lane's
+ * run of at most sigma (4 or 8) consecutive products of a row is summed by an
+ * FP32 fused multiply-add chain and widened to FP64 once; the warp scan, the
+ * carries and the alpha/beta update stay FP64.  Per row the error against the
+ * FP64 inputs is at most about 10 * 2^-24 (6e-7) of sum_j |a_ij x_j|.  Tiled
+ * kernel only (cfg NULL or kernel SBB_KERNEL_AUTO / SBB_KERNEL_TILED,
+ * tile_sigma 0 = 8, or 4); anything else is SBB_ERR_ARG.  Run it with
+ * sbb_spmv_f32.  No counterpart in the reference (it has no FP32 path). */
+int sbb_plan_create_f32_lanes(sbb_plan_t *plan, int m, int n, int nnz,
+                              const int *d_rowptr, const int *d_col,
+                              const float *d_val, const sbb_config *cfg, void *stream);
 /* y = alpha*A*x + beta*y on the stream (asynchronous).  y is not read when
  * beta == 0.  Out-of-range column indices are skipped and flagged; see
  * sbb_plan_check.  x (n values) and y (m values) must not overlap

@@ -214,6 +214,17 @@ static int plan_build_impl(Plan *p, const sbb_config *cfg, cudaStream_t s, bool 
     if (c.vector_width) vw = c.vector_width;
     if (c.items_per_thread) ipt = c.items_per_thread;
     if (c.tile_sigma) sigma = c.tile_sigma;
+    if (p->lane32) {
+        // FP32 lane sums exist in the tiled kernel only, for runs of at most
+        // 8 products per lane (the error bound of the form)
+        if (c.kernel == SBB_KERNEL_AUTO) k = SBB_KERNEL_TILED;
+        if (!c.tile_sigma) sigma = 8;
+        if (k != SBB_KERNEL_TILED || (sigma != 4 && sigma != 8) || p->m > kTiledMaxRows) {
+            set_error("FP32 lane sums need the tiled kernel with tile_sigma 4 or 8 "
+                      "(and at most 2^31 - 1025 rows)");
+            return SBB_ERR_ARG;
+        }
+    }
     p->kernel = k;
     p->vector_width = vw;
     p->ipt = ipt;
@@ -366,7 +377,8 @@ struct sbb_plan_s {
 };
 
 static int create_common(sbb_plan_t *out, int m, int n, int nnz, const int *rp, const int *col,
-                         const void *val, bool f32, const sbb_config *cfg, void *stream)
+                         const void *val, bool f32, const sbb_config *cfg, void *stream,
+                         bool lane32 = false)
 {
     if (!out) {
         set_error("plan pointer is NULL");
@@ -385,6 +397,7 @@ static int create_common(sbb_plan_t *out, int m, int n, int nnz, const int *rp, 
     h->p.col = col;
     h->p.val = val;
     h->p.f32 = f32;
+    h->p.lane32 = lane32;
     int rc = plan_build(&h->p, cfg, static_cast<cudaStream_t>(stream));
     if (rc != SBB_OK) {
         cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
@@ -409,6 +422,13 @@ int sbb_plan_create_f32(sbb_plan_t *plan, int m, int n, int nnz, const int *d_ro
                         void *stream)
 {
     return create_common(plan, m, n, nnz, d_rowptr, d_col, d_val, true, cfg, stream);
+}
+
+int sbb_plan_create_f32_lanes(sbb_plan_t *plan, int m, int n, int nnz, const int *d_rowptr,
+                              const int *d_col, const float *d_val, const sbb_config *cfg,
+                              void *stream)
+{
+    return create_common(plan, m, n, nnz, d_rowptr, d_col, d_val, true, cfg, stream, true);
 }
 
 // x (n values) overlapping y (m doubles): an error, set here.

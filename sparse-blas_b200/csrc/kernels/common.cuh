@@ -106,6 +106,21 @@ struct AccF32 {
     __device__ __forceinline__ void mac(float v, float x) { s = __fma_rn((double)v, (double)x, s); }
     __device__ __forceinline__ double get() const { return s; }
 };
+// FP32 lane sums (the tiled kernel only, sigma <= 8): a lane's run of at
+// most sigma consecutive products of one row is summed by an FP32 fma chain
+// and widened to FP64 once, where the warp scan, the carries and the alpha /
+// beta update take over.  A run of k <= 8 terms is within k * 2^-24 of its
+// exact sum relative to sum |v*x| (the chain's first step rounds the
+// product, each later one the running sum); with the rounding of val and x
+// to float that bounds a row's error by 10 * 2^-24 ~ 6e-7 of sum_j |a_ij x_j|.
+// Per nnz: one FP32 fma instead of two float-to-double conversions and an
+// FP64 fma.
+struct AccF32Lane {
+    float s;
+    __device__ __forceinline__ void zero() { s = 0.0f; }
+    __device__ __forceinline__ void mac(float v, float x) { s = __fmaf_rn(v, x, s); }
+    __device__ __forceinline__ double get() const { return (double)s; }
+};
 
 // The y update alpha*sum + beta*y as fma(alpha, sum, beta*y); alpha*sum
 // alone when beta == 0 (y is then not read: the cuSPARSE convention).  The

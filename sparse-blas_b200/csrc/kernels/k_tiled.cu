@@ -37,6 +37,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 
+#include <type_traits>
+
 #include <cub/cub.cuh>
 
 #include "../sbb_internal.h"
@@ -428,8 +430,16 @@ void launch_tiled_t(const TiledPlan &T, int m, int n, long long nnz, double alph
         switch (T.sigma) {
         case 4: launch_tiled_s<PT, ACC, 4>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
         case 8: launch_tiled_s<PT, ACC, 8>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
-        case 16: launch_tiled_s<PT, ACC, 16>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
-        case 32: launch_tiled_s<PT, ACC, 32>(T, m, n, nnz, alpha, x, beta, y, status, s); break;
+        case 16:
+        case 32:
+            // FP32 lane sums are built for runs of at most 8 products
+            if constexpr (!std::is_same<ACC, AccF32Lane>::value) {
+                if (T.sigma == 16)
+                    launch_tiled_s<PT, ACC, 16>(T, m, n, nnz, alpha, x, beta, y, status, s);
+                else
+                    launch_tiled_s<PT, ACC, 32>(T, m, n, nnz, alpha, x, beta, y, status, s);
+            }
+            break;
         default: break;
         }
         launch_fixup(m, T.carry_row, T.carry_val, T.tiles, T.runs, alpha, y, nullptr, s);
@@ -556,7 +566,10 @@ int tiled_run(Plan *p, double alpha, const void *x, double beta, double *y, cuda
         set_error("tiled plan missing");
         return SBB_ERR_ARG;
     }
-    if (p->f32)
+    if (p->f32 && p->lane32)
+        launch_tiled_t<ProdF32, AccF32Lane>(*T, p->m, p->n, p->nnz, alpha,
+                                            static_cast<const float *>(x), beta, y, p->status, s);
+    else if (p->f32)
         launch_tiled_t<ProdF32, AccF32>(*T, p->m, p->n, p->nnz, alpha,
                                         static_cast<const float *>(x), beta, y, p->status, s);
     else

@@ -260,6 +260,7 @@ struct Plan {
     const int *rowptr = nullptr, *col = nullptr;
     const void *val = nullptr;
     bool f32 = false;
+    bool lane32 = false;     // FP32 storage summed in FP32 lane runs (tiled, sigma <= 8)
     int kernel = 0;          // resolved SBB_KERNEL_*
     int vector_width = 0;    // K1
     int ipt = 0;             // K2

@@ -69,6 +69,8 @@ SIGNATURES = {
                                   C.POINTER(Config), vp]),
     "sbb_plan_create_f32": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.c_int, vp, vp, vp,
                                       C.POINTER(Config), vp]),
+    "sbb_plan_create_f32_lanes": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.c_int, vp, vp,
+                                            vp, C.POINTER(Config), vp]),
     "sbb_spmv": (C.c_int, [vp, C.c_double, vp, C.c_double, vp, vp]),
     "sbb_spmv_f32": (C.c_int, [vp, C.c_double, vp, C.c_double, vp, vp]),
     "sbb_spmv_timed": (C.c_int, [vp, C.c_double, vp, C.c_double, vp, vp, vp, vp]),

@@ -31,11 +31,14 @@ class Plan:
     """A reusable SpMV plan for one CSR matrix resident on the GPU.
 
     rowptr/col are int32 CUDA tensors, val float64 (or float32 with f32=True).
-    The tensors are kept alive by the plan.
+    f32_lanes=True (with f32=True) builds the FP32-storage form whose lane
+    runs of at most 8 products are summed in FP32 (sbb_plan_create_f32_lanes;
+    tiled kernel only).  The tensors are kept alive by the plan.
     """
 
     def __init__(self, rowptr, col, val, n, kernel="auto", vector_width=0,
-                 items_per_thread=0, persistent=0, tile_sigma=0, f32=False, stream=None):
+                 items_per_thread=0, persistent=0, tile_sigma=0, f32=False, stream=None,
+                 f32_lanes=False):
         import torch
         assert rowptr.dtype == torch.int32 and col.dtype == torch.int32
         assert val.dtype == (torch.float32 if f32 else torch.float64)
@@ -47,7 +50,9 @@ class Plan:
         cfg = Config(KERNELS[kernel] if isinstance(kernel, str) else int(kernel),
                      vector_width, items_per_thread, persistent, tile_sigma)
         h = C.c_void_p()
-        create = lib().sbb_plan_create_f32 if f32 else lib().sbb_plan_create
+        assert f32 or not f32_lanes
+        create = (lib().sbb_plan_create_f32_lanes if f32_lanes else
+                  lib().sbb_plan_create_f32 if f32 else lib().sbb_plan_create)
         rc = create(C.byref(h), self.m, self.n, self.nnz, _ptr(rowptr), _ptr(col), _ptr(val),
                     C.byref(cfg), _stream(stream))
         if rc != 0:
