@@ -118,18 +118,27 @@ def test_memory_precheck_returns_minus_1(hooks, version):
     _check_ok(version, rp, col, val, x, y)
 
 
-def test_tiled_wait_timeout_reports_status(hooks):
+@pytest.mark.parametrize("form", ["fp64", "f32", "f32_lanes"])
+def test_tiled_wait_timeout_reports_status(hooks, form):
     """A zero poll budget for the first tile-copy wait of the first warp: the
     kernel gives up that wait, lets its copies in flight land, raises the
     timeout status and stops; sbb_plan_check reports SBB_ERR_INPUT with the
-    timeout message, and the context stays usable."""
+    timeout message, and the context stays usable.  fp64: 32 x 4 tiles, a
+    two-tile ring; f32 / f32_lanes: the FP32-storage 32 x 8 tiles, a
+    three-tile ring with the x gathers one tile ahead."""
     import torch
+    from helpers import TOL_FP32
     from sbb._lib import TEST_RESET, TEST_WAIT_BUDGET
     from sbb.device import Plan, SbbError
     rp, col, val, x, y = _case(seed=42, m=60000, n=50000, lmax=40)
     d = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a)).to("cuda:0", dt)  # noqa: E731
-    drp, dcol, dval, dx = d(rp.astype(np.int32)), d(col), d(val), d(x)
-    P = Plan(drp, dcol, dval, len(x), kernel="tiled", tile_sigma=4)
+    f32 = form != "fp64"
+    drp, dcol = d(rp.astype(np.int32)), d(col)
+    dval = d(val.astype(np.float32)) if f32 else d(val)
+    dx = d(x.astype(np.float32)) if f32 else d(x)
+    kw = dict(kernel="tiled", tile_sigma=8 if f32 else 4, f32=f32,
+              f32_lanes=form == "f32_lanes")
+    P = Plan(drp, dcol, dval, len(x), **kw)
     assert hooks.sbb_test_hook(TEST_WAIT_BUDGET, 0) == 0
     yd = d(y)
     P.spmv(dx, yd, 1.5, -0.5)
@@ -139,14 +148,14 @@ def test_tiled_wait_timeout_reports_status(hooks):
         P.check()
     P.close()
     # a fresh plan on the same context computes the right result
-    P = Plan(drp, dcol, dval, len(x), kernel="tiled", tile_sigma=4)
+    P = Plan(drp, dcol, dval, len(x), **kw)
     yd = d(y)
     P.spmv(dx, yd, 1.5, -0.5)
     torch.cuda.synchronize()
     P.check()
     P.close()
     y_ref, scale = O.spmv_dd(rp, col, val, x, 1.5, -0.5, y)
-    assert max_scaled_err(yd.cpu().numpy(), y_ref, scale) <= TOL_FP64
+    assert max_scaled_err(yd.cpu().numpy(), y_ref, scale) <= (TOL_FP32 if f32 else TOL_FP64)
 
 
 def test_dropin_kernel3_timeout_returns_minus_1(hooks):
