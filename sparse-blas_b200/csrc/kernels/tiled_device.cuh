@@ -197,38 +197,35 @@ __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
     double head = 0.0;
     bool started = false;
     int seg = head_seg;
-    auto vals = [&](int g, V (&v)[4]) {
-        if constexpr (sizeof(V) == 8) {
-            double2 a = *reinterpret_cast<const double2 *>(s_val + g * 128 + lane * 2);
-            double2 b = *reinterpret_cast<const double2 *>(s_val + g * 128 + 64 + lane * 2);
-            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-        } else {
-            float4 a = *reinterpret_cast<const float4 *>(s_val + g * 128 + lane * 4);
-            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-        }
-    };
-    auto general = [&]() {  // any number of row starts per lane
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            V v[4];
-            vals(g, v);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int s = g * 4 + j;
-                if ((bits >> s) & 1u) {
-                    if (!started) {
-                        head = acc.get();
-                        started = true;
-                    } else {  // a whole row inside this lane
-                        put(seg, acc.get());
-                    }
-                    acc.zero();
-                    ++seg;
-                }
-                acc.mac(v[j], xv[s]);
-            }
-        }
-    };
+    // The general loop: any number of row starts per lane.
+#define SBB_TILE_GENERAL_LOOP()                                                                   \
+    _Pragma("unroll") for (int g = 0; g < G; ++g)                                                 \
+    {                                                                                             \
+        V v[4];                                                                                   \
+        if constexpr (sizeof(V) == 8) {                                                           \
+            double2 a = *reinterpret_cast<const double2 *>(s_val + g * 128 + lane * 2);           \
+            double2 b = *reinterpret_cast<const double2 *>(s_val + g * 128 + 64 + lane * 2);      \
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;                                       \
+        } else {                                                                                  \
+            float4 a = *reinterpret_cast<const float4 *>(s_val + g * 128 + lane * 4);             \
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;                                       \
+        }                                                                                         \
+        _Pragma("unroll") for (int j = 0; j < 4; ++j)                                             \
+        {                                                                                         \
+            const int s = g * 4 + j;                                                              \
+            if ((bits >> s) & 1u) {                                                               \
+                if (!started) {                                                                   \
+                    head = acc.get();                                                             \
+                    started = true;                                                               \
+                } else { /* a whole row inside this lane */                                       \
+                    put(seg, acc.get());                                                          \
+                }                                                                                 \
+                acc.zero();                                                                       \
+                ++seg;                                                                            \
+            }                                                                                     \
+            acc.mac(v[j], xv[s]);                                                                 \
+        }                                                                                         \
+    }
     // FP32 storage with exact FP64 products: when no lane of the warp starts
     // two rows (every row here is longer than sigma, as in banded matrices),
     // a lane's products before its row start (if any) go to h and the rest
@@ -244,8 +241,8 @@ __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
             h.zero();
 #pragma unroll
             for (int g = 0; g < G; ++g) {
-                V v[4];
-                vals(g, v);
+                const float4 a = *reinterpret_cast<const float4 *>(s_val + g * 128 + lane * 4);
+                const float v[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     if (g * 4 + j < p1)
@@ -262,11 +259,12 @@ __device__ __forceinline__ void tile_reduce(int t, const unsigned char *tb,
                 acc = h;
             }
         } else {
-            general();
+            SBB_TILE_GENERAL_LOOP()
         }
     } else {
-        general();
+        SBB_TILE_GENERAL_LOOP()
     }
+#undef SBB_TILE_GENERAL_LOOP
 
     // 4. warp segmented scan of lane carries, reset at lanes that start a row
     // A lane adds the partial scan from o lanes back while no row starts in
